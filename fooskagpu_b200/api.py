@@ -1,0 +1,205 @@
+"""Python host API over the C ABI (mirrors the reference's stage functions).
+
+    mesh = Mesh.load_neu("sh.neu", scale=1e-3)
+    case = default_case(); case.rkSteps = 3
+    s = Solver(mesh, case, precision="mixed")
+    s.set_state(U)          # initialize / readField
+    s.step()                # one explicitLoop iteration
+    U = s.get_state()
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import FgCase, FgMeshInfo, FgMeshOpts, FgMeshView, FgRelaxStats, check, lib
+
+_PREC = {"fp64": L.FG_PREC_FP64, "mixed": L.FG_PREC_MIXED}
+_RENUM = {"none": L.FG_RENUMBER_NONE, "morton": L.FG_RENUMBER_MORTON, "rcm": L.FG_RENUMBER_RCM}
+
+
+def default_case() -> FgCase:
+    """The parameters the reference hard-codes in DP/buildInput.cu:10-69."""
+    c = FgCase()
+    lib().fg_case_default(C.byref(c))
+    return c
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(L.PD)
+
+
+class Mesh:
+    """Pre-processed mesh (reference face order + device renumbering)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        info = FgMeshInfo()
+        check(lib().fg_mesh_info_get(self._h, C.byref(info)))
+        self.info = {k: getattr(info, k) for k, _ in FgMeshInfo._fields_}
+        self.n_elem = info.nElem
+        self.n_fcs = info.nFcs
+
+    @classmethod
+    def load_neu(cls, path: str, scale: float = 1.0, periodic=(0.0, 0.0, 0.0), renumber: str = "morton") -> "Mesh":
+        o = FgMeshOpts()
+        o.scale = scale
+        for d in range(3):
+            o.periodic[d] = periodic[d]
+        o.renumber = _RENUM[renumber]
+        h = C.c_void_p()
+        check(lib().fg_mesh_load_neu(path.encode(), C.byref(o), C.byref(h)))
+        return cls(h)
+
+    def view(self) -> FgMeshView:
+        v = FgMeshView()
+        check(lib().fg_mesh_view_get(self._h, C.byref(v)))
+        return v
+
+    def arrays(self) -> dict:
+        """Copies of the reference-layout mesh arrays (numpy)."""
+        v = self.view()
+        nE, nF = v.nElem, v.nFcs
+        g = lambda p, k, dt=np.float64: np.ctypeslib.as_array(p, shape=(k,)).astype(dt).copy()
+        return {
+            "fc2el": g(v.fc2el, 2 * nF, np.int32).reshape(nF, 2),
+            "boundCond": g(v.boundCond, nF, np.int32),
+            "cellCenter": g(v.cellCenter, 3 * nE).reshape(nE, 3),
+            "fcCenter": g(v.fcCenter, 3 * nF).reshape(nF, 3),
+            "n": g(v.n, 3 * nF).reshape(nF, 3),
+            "nt1": g(v.nt1, 3 * nF).reshape(nF, 3),
+            "nt2": g(v.nt2, 3 * nF).reshape(nF, 3),
+            "area": g(v.area, nF),
+            "volume": g(v.volume, nE),
+            "nbShift": g(v.nbShift, 3 * nF).reshape(nF, 3),
+        }
+
+    def permutation(self) -> np.ndarray:
+        p = np.empty(self.n_elem, dtype=np.int32)
+        check(lib().fg_mesh_permutation(self._h, p.ctypes.data_as(L.PI), self.n_elem))
+        return p
+
+    def close(self):
+        if self._h:
+            lib().fg_mesh_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """Device solver for one mesh and case; all state lives in HBM."""
+
+    def __init__(self, mesh: Mesh, case: FgCase, precision: str = "mixed", device: int = 0):
+        self.mesh = mesh
+        self.case = case
+        self.precision = precision
+        h = C.c_void_p()
+        check(lib().fg_solver_create(mesh._h, C.byref(case), _PREC[precision], device, C.byref(h)))
+        self._h = h
+        self.n = mesh.n_elem
+
+    # -- state
+    def set_state(self, U: np.ndarray, stream: Optional[int] = None) -> None:
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.n, 10)
+        check(lib().fg_set_state(self._h, _dptr(U), stream))
+
+    def get_state(self, out: Optional[np.ndarray] = None, stream: Optional[int] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.n, 10), dtype=np.float64)
+        check(lib().fg_get_state(self._h, _dptr(out), stream))
+        return out
+
+    # -- stage functions
+    def compute_rhs(self, want_signal: bool = False, stream=None) -> None:
+        check(lib().fg_compute_rhs(self._h, 1 if want_signal else 0, stream))
+
+    def compute_time_step(self, stream=None) -> float:
+        dt = C.c_double()
+        check(lib().fg_compute_time_step(self._h, C.byref(dt), stream))
+        return dt.value
+
+    def init_rk(self, stream=None) -> None:
+        check(lib().fg_init_rk(self._h, stream))
+
+    def update(self, irk: int, stream=None) -> None:
+        check(lib().fg_update(self._h, irk, stream))
+
+    def stage(self, irk: int, stream=None) -> None:
+        check(lib().fg_stage(self._h, irk, stream))
+
+    def relaxation(self, stream=None) -> dict:
+        st = FgRelaxStats()
+        check(lib().fg_relaxation(self._h, C.byref(st), stream))
+        return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort}
+
+    def cons_calc(self, ivar: int, stream=None) -> float:
+        v = C.c_double()
+        check(lib().fg_cons_calc(self._h, ivar, C.byref(v), stream))
+        return v.value
+
+    def step(self, stream=None) -> None:
+        check(lib().fg_step(self._h, stream))
+
+    def time(self):
+        dt, t, it = C.c_double(), C.c_double(), C.c_int32()
+        check(lib().fg_get_time(self._h, C.byref(dt), C.byref(t), C.byref(it)))
+        return dt.value, t.value, it.value
+
+    def set_dt(self, dt: float) -> None:
+        check(lib().fg_set_dt(self._h, float(dt)))
+
+    def memory_bytes(self) -> int:
+        b = C.c_uint64()
+        check(lib().fg_solver_memory(self._h, C.byref(b)))
+        return b.value
+
+    # -- instrumentation
+    def profile(self, enable: bool = True) -> None:
+        check(lib().fg_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        t = L.FgKernelTimes()
+        check(lib().fg_profile_read(self._h, C.byref(t)))
+        return {k: {"ms": t.ms[i], "launches": int(t.launches[i])} for i, k in enumerate(L.KERNEL_KINDS)
+                if t.launches[i] > 0}
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        check(lib().fg_launch_count(self._h, C.byref(v)))
+        return int(v.value)
+
+    # -- parity hooks
+    def get_rhs(self) -> np.ndarray:
+        out = np.empty((self.n, 10))
+        check(lib().fg_get_rhs(self._h, _dptr(out)))
+        return out
+
+    def get_limited(self):
+        g = np.empty((self.n, 10, 3))
+        th = np.empty((self.n, 10))
+        check(lib().fg_get_limited(self._h, _dptr(g), _dptr(th)))
+        return g, th
+
+    def get_signal(self) -> np.ndarray:
+        out = np.empty(self.n)
+        check(lib().fg_get_signal(self._h, _dptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fg_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,96 @@
+"""Build recipe for the native libraries (nvcc / g++ invoked directly, outputs in-tree).
+
+* ``fooskagpu_b200/libfooskagpu.so`` — the product: CUDA kernels for sm_100a + host C++ and
+  the C ABI declared in ``include/fooskagpu.h``.
+* ``oracle/liboracle.so`` — the CPU FP64 restatement used by tests and the CPU baseline.
+
+Each target is rebuilt only when one of its sources is newer than the output.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+PKG = ROOT / "fooskagpu_b200"
+CSRC = PKG / "csrc"
+LIB = PKG / "libfooskagpu.so"
+ORACLE_DIR = ROOT / "oracle"
+ORACLE_LIB = ORACLE_DIR / "liboracle.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(out: Path, srcs) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(Path(s).stat().st_mtime > t for s in srcs)
+
+
+def _run(cmd, cwd=None):
+    r = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed:\n" + " ".join(map(str, cmd)) + "\n" + r.stdout + r.stderr)
+    return r.stdout + r.stderr
+
+
+def build_product(force: bool = False, verbose: bool = False) -> Path:
+    cu = [CSRC / "fg_kernels.cu", CSRC / "fg_relax.cu", CSRC / "fg_solver.cu"]
+    cpp = [CSRC / "fg_mesh.cpp"]
+    hdr = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "fooskagpu.h"]
+    if not force and not _stale(LIB, cu + cpp + hdr):
+        return LIB
+    objdir = ROOT / "_build"
+    objdir.mkdir(exist_ok=True)
+    nvcc = _nvcc()
+    objs = []
+    common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-I", str(ROOT / "include")]
+    for s in cu:
+        o = objdir / (s.stem + ".o")
+        cmd = [nvcc, *ARCH, "-lineinfo", *common, "-c", str(s), "-o", str(o)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        out = _run(cmd)
+        if verbose and out:
+            print(out)
+        objs.append(o)
+    for s in cpp:
+        o = objdir / (s.stem + ".o")
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", str(ROOT / "include"), "-c", str(s), "-o", str(o)])
+        objs.append(o)
+    tmp = LIB.with_suffix(".so.tmp")
+    _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def build_oracle(force: bool = False) -> Path:
+    src = [ORACLE_DIR / "oracle.cpp", ORACLE_DIR / "oracle.h", ROOT / "include" / "fooskagpu.h"]
+    if not force and not _stale(ORACLE_LIB, src):
+        return ORACLE_LIB
+    tmp = ORACLE_LIB.with_suffix(".so.tmp")
+    _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+          "-I", str(ROOT / "include"), str(ORACLE_DIR / "oracle.cpp"), "-o", str(tmp)])
+    os.replace(tmp, ORACLE_LIB)
+    return ORACLE_LIB
+
+
+def build_all(force: bool = False, verbose: bool = False) -> None:
+    build_product(force=force, verbose=verbose)
+    build_oracle(force=force)
+
+
+if __name__ == "__main__":
+    import sys
+    build_all(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print("built", LIB, ORACLE_LIB)

@@ -1,0 +1,148 @@
+"""Case parameters (``fg_case`` = the reference's INPUT fields) and initial conditions.
+
+Initial states are built like the reference's initVec (DP/initialize.cu:18-59): phasic
+densities from (p, T) or given directly, phasic internal energies from the stiffened-gas
+e(p, rho), and U = [alpha, alpha rhoL, (1-alpha) rhoG, rho u, rho v, rho w,
+alpha rhoL eL, (1-alpha) rhoG eG, rho E, m_v].
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .api import default_case
+from ._lib import FgCase
+
+
+def _e(case: FgCase, m: int, p, rho):
+    g, pinf, eta = case.gamma[m], case.pInf[m], case.eta[m]
+    return (p + g * pinf + (g - 1) * eta * rho) / (rho * (g - 1))
+
+
+def rho_of_pT(case: FgCase, m: int, p, T):
+    g, pinf, cp = case.gamma[m], case.pInf[m], case.Cp[m]
+    return (p + pinf) / ((cp / g) * T * (g - 1))
+
+
+def prim_to_cons(case: FgCase, alpha, rhoL, rhoG, u, v, w, pL, pG=None, mv=0.0) -> np.ndarray:
+    alpha, rhoL, rhoG, u, v, w, pL = np.broadcast_arrays(*map(np.asarray, (alpha, rhoL, rhoG, u, v, w, pL)))
+    pG = pL if pG is None else np.broadcast_to(np.asarray(pG), pL.shape)
+    mv = np.broadcast_to(np.asarray(mv, dtype=np.float64), pL.shape)
+    n = pL.shape[0]
+    U = np.empty((n, 10))
+    ar = alpha * rhoL
+    ag = (1 - alpha) * rhoG
+    rho = ar + ag
+    eL = _e(case, 0, pL, rhoL)
+    eG = _e(case, 1, pG, rhoG)
+    U[:, 0] = alpha
+    U[:, 1] = ar
+    U[:, 2] = ag
+    U[:, 3] = rho * u
+    U[:, 4] = rho * v
+    U[:, 5] = rho * w
+    U[:, 6] = ar * eL
+    U[:, 7] = ag * eG
+    U[:, 8] = ar * eL + ag * eG + 0.5 * rho * (u * u + v * v + w * w)
+    U[:, 9] = mv
+    return U
+
+
+# ---------------------------------------------------------------- single-phase ideal gas
+def ideal_gas_case(gamma=1.4, cp=3.5, mu=0.0, rk=3, cfl=0.5, adapt_itr=100) -> FgCase:
+    """Both phases the same ideal gas (p_inf = 0, eta = 0, equal Cp), no phase change:
+    the two-phase model then reduces to single-phase Euler/Navier-Stokes for any alpha."""
+    c = default_case()
+    for m in range(2):
+        c.gamma[m] = gamma
+        c.pInf[m] = 0.0
+        c.Cp[m] = cp
+        c.eta[m] = 0.0
+        c.dynVisc[m] = mu
+        c.satConst[m] = 0.0
+    c.chemFlag = 0
+    c.woodsFlag = 0
+    c.viscFlag = 1 if mu > 0 else 0
+    c.turbulence = 1 if mu > 0 else 0
+    c.rkSteps = rk
+    c.cfl = cfl
+    c.maxDt = 1e30
+    c.adaptDt = 1
+    c.adaptDtItr = adapt_itr
+    c.scale = 1.0
+    c.consCalcIvar = 1
+    return c
+
+
+def sod_case() -> FgCase:
+    """Sod shock tube (inviscid HLLC + MUSCL, SSP-RK3, CFL 0.5)."""
+    return ideal_gas_case(gamma=1.4, cp=3.5, mu=0.0, rk=3, cfl=0.5, adapt_itr=10)
+
+
+def sod_ic(case: FgCase, centres: np.ndarray, x0: float = 0.5, alpha: float = 0.5) -> np.ndarray:
+    left = centres[:, 0] < x0
+    rho = np.where(left, 1.0, 0.125)
+    p = np.where(left, 1.0, 0.1)
+    z = np.zeros_like(rho)
+    return prim_to_cons(case, alpha, rho, rho, z, z, z, p)
+
+
+def tgv_case(mach=0.1, re=1600.0, rk=3, cfl=0.5) -> FgCase:
+    """Taylor-Green vortex, rho0 = V0 = L = 1, mu = rho0 V0 L / Re, WALE LES."""
+    return ideal_gas_case(gamma=1.4, cp=3.5, mu=1.0 / re, rk=rk, cfl=cfl, adapt_itr=100)
+
+
+def tgv_ic(case: FgCase, centres: np.ndarray, mach=0.1, alpha: float = 0.5) -> np.ndarray:
+    x, y, z = centres[:, 0], centres[:, 1], centres[:, 2]
+    g = case.gamma[0]
+    p0 = 1.0 / (g * mach * mach)
+    u = np.sin(x) * np.cos(y) * np.cos(z)
+    v = -np.cos(x) * np.sin(y) * np.cos(z)
+    w = np.zeros_like(x)
+    p = p0 + (1.0 / 16.0) * (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0)
+    rho = p / p0                     # isothermal start
+    return prim_to_cons(case, alpha, rho, rho, u, v, w, p)
+
+
+# ---------------------------------------------------------------- the reference's own case
+def reference_case() -> FgCase:
+    """The parameters hard-coded in DP/buildInput.cu:10-69 with mesh coordinates in metres."""
+    c = default_case()
+    c.scale = 1.0
+    return c
+
+
+def reference_ic(case: FgCase, centres: np.ndarray) -> np.ndarray:
+    """Two regions split at x < 0 (DP/initialize.cu:4-8, 26): liquid at 11.4e5 Pa / 115.3 K on
+    the left, vapour at 2.6e5 Pa / 115.3 K on the right."""
+    left = centres[:, 0] < 0.0
+    alpha = np.where(left, 1.0 - case.avfMin, case.avfMin)
+    p = np.where(left, 11.4e5, 2.6e5)
+    T = 115.3
+    rl = rho_of_pT(case, 0, p, T)
+    rg = rho_of_pT(case, 1, p, T)
+    z = np.zeros_like(p)
+    return prim_to_cons(case, alpha, rl, rg, z, z, z, p)
+
+
+def perturbed_two_phase_ic(case: FgCase, centres: np.ndarray, seed: int = 7, vel=20.0) -> np.ndarray:
+    """Smoothly varying two-phase state around the reference's operating point: volume
+    fraction, pressures and temperatures vary in space, velocities of O(vel), some cells
+    above saturation and some with vapour mass above chemLimit (exercises Wood's sound
+    speed, star states of both signs and the chemical relaxation branch)."""
+    rng = np.random.default_rng(seed)
+    x = centres
+    span = np.ptp(x, axis=0) + 1e-30
+    xi = (x - x.min(axis=0)) / span
+    k = rng.uniform(1.0, 3.0, size=(6, 3))
+    ph = rng.uniform(0, 2 * np.pi, size=6)
+    f = [np.sin(2 * np.pi * (xi @ k[i]) + ph[i]) for i in range(6)]
+    alpha = 0.5 + 0.45 * f[0]
+    p = 7e5 + 4e5 * f[1]
+    T = 115.3 + 3.0 * f[2]
+    rl = rho_of_pT(case, 0, p, T)
+    rg = rho_of_pT(case, 1, p, T)
+    u = vel * f[3]
+    v = vel * f[4]
+    w = vel * 0.5 * f[5]
+    mv = (1 - alpha) * rg * np.clip(0.5 + 0.5 * f[0], 0, 1)
+    return prim_to_cons(case, alpha, rl, rg, u, v, w, p, p, mv)

@@ -1,0 +1,75 @@
+// Kernel argument structs and launcher declarations shared by fg_kernels.cu and fg_solver.cu.
+#pragma once
+#include "fg_device.cuh"
+
+namespace fg {
+
+// Cell-ordered (renumbered) device mesh.  Per-slot arrays are slot-major: a[k * n + c].
+template <typename T>
+struct DevMesh {
+    int n;              // cells
+    int nSlots;         // max faces per cell
+    const int32_t *nbr;   // neighbour cell, or -bc (1..5) on a boundary slot, or INT32_MIN unused
+    const int32_t *flags; // bits 0-2: faces of the cell; bit 3+k: cell owns the face of slot k
+    const T *nx, *ny, *nz, *A;       // canonical (owner -> neighbour) unit normal and area
+    const T *dcx, *dcy, *dcz;        // face centre - own cell centre
+    const T *dnx, *dny, *dnz;        // face centre - neighbour cell centre (periodic image)
+    const double *vol;               // cell volume
+    const double *volP;              // pow(vol, 0.3333) as the reference's CFL bound uses
+};
+
+template <typename T>
+struct Fields {
+    double *U;          // [10][n]
+    double *U0;         // [10][n]
+    double *RHS;        // [10][n] (RHS-mode residual)
+    T *Win;             // [n][WREC] primitive record read this stage
+    T *Wout;            // [n][WREC] primitive record written this stage
+    T *G;               // [n][GREC] limiter + gradient
+    double *signal;     // [n]
+    double *blockMin;   // [nBlocks]
+    double *dt;         // device scalar
+};
+
+enum FluxMode { FLUX_FUSED = 0, FLUX_RHS = 1 };
+
+struct StageCoef {
+    int rk;        // 1 (forward Euler) or 3 (SSP-RK3, Shu-Osher)
+    int irk;       // stage
+    int writeU0;   // stage 0 of RK3 also stores U0 = U
+    int neglectZ;  // the reference's only effective neglect flag (DP/update.cu:26-28)
+};
+
+template <typename T>
+void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cudaStream_t s);
+template <typename T>
+void launch_flux(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, const PhysD &D,
+                 int mode, int wantSignal, StageCoef sc, cudaStream_t s);
+template <typename T>
+void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, StageCoef sc, cudaStream_t s);
+template <typename T>
+void launch_prim(int n, const double *U, T *W, const PhysD &D, cudaStream_t s);
+// dt = min(cfl * min_blocks, maxDt) from blockMin[nBlocks]
+void launch_dt_finalize(const double *blockMin, int nBlocks, double cfl, double maxDt, double *dt, cudaStream_t s);
+int flux_blocks(int n);
+
+// relaxation (FP64 Newton), writes U and the primitive record
+struct RelaxParams {
+    double gam[2], pinf[2], cp[2], eta[2], satConst[2];
+    double avfMin, chemLimit, thermUrf, chemUrf, satTempUrf;
+    int thermItrMax, chemItrMax, chemFlag;
+};
+template <typename T>
+void launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
+                  cudaStream_t s);
+
+// conservation integral: blockSum then ordered final sum into out
+void launch_cons(int n, int ivar, const double *U, const double *vol, double *blockSum, double *out, cudaStream_t s);
+int cons_blocks(int n);
+
+// reference-order AoS <-> renumbered SoA
+void launch_scatter_state(int n, const double *Uaos, const int32_t *new2old, double *U, cudaStream_t s);
+void launch_gather_state(int n, const double *U, const int32_t *new2old, double *Uaos, cudaStream_t s);
+void launch_copy_u0(int n, const double *U, double *U0, cudaStream_t s);
+
+}  // namespace fg

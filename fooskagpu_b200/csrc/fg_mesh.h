@@ -1,0 +1,54 @@
+// Host-side mesh: Gambit neutral reader, face matching, reference geometry, renumbering.
+#pragma once
+#include "../../include/fooskagpu.h"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace fg {
+
+// Per-element-type local face tables (Gambit node numbering).
+//  kFaceNodesCentre: node order the reference uses to average face centres (DP/translator.cu:146-280)
+//  kFaceNodesGeom:   node order the reference uses for normals/areas (DP/operations.h:15-49)
+struct ElemType {
+    int nNodes;          // 4 tet, 5 pyramid, 6 prism, 8 hex
+    int nFaces;
+    int faceNodeCount[6];
+    int centreNodes[6][4];
+    int geomNodes[6][4];
+    int volTets;         // tetra split for the volume (DP/meshProperties.cu:168-171)
+    int volNodes[6][3];
+};
+const ElemType *elem_type_for_nodes(int nNodes);
+
+struct Mesh {
+    // ---- reference layout (.neu order) ----
+    int nElem = 0, nNodes = 0, nFcs = 0;
+    std::vector<double> nodes;         // nNodes*3, scaled
+    std::vector<int32_t> elNodes;      // nElem*8
+    std::vector<int32_t> elNN;         // nodes per element
+    std::vector<int32_t> elBc;         // nElem*6 boundary code per local face
+    std::vector<double> cellCenter;    // nElem*3
+    std::vector<double> elFcCenter;    // nElem*18
+    std::vector<int32_t> neig, neigFc; // nElem*6, -1 on boundary
+    std::vector<double> neigShift;     // nElem*18 periodic image offset of the neighbour face
+    std::vector<int32_t> fc2el, fc2elFc, boundCond;
+    std::vector<double> fcCenter, n, nt1, nt2, area, volume, nbShift;
+    int nBoundary = 0, nPeriodic = 0, maxFaces = 0;
+    int nTet = 0, nPyr = 0, nPrism = 0, nHex = 0;
+    // ---- device ordering ----
+    std::vector<int32_t> new2old, old2new;
+};
+
+// Parse a Gambit neutral file with the reference's grammar (DP/translator.cu:3-354).
+// Returns FG_OK or an error code with a message in err.
+int read_neu(const std::string &path, double scale, Mesh &m, std::string &err);
+// Match faces, build the reference face order and geometry, renumber.
+int finish_mesh(Mesh &m, const fg_mesh_opts &o, std::string &err);
+
+}  // namespace fg
+
+struct fg_mesh {
+    fg::Mesh m;
+};

@@ -1,0 +1,318 @@
+// Phase relaxation (FP64): partition by saturation temperature, thermal (p, T) equilibrium
+// Newton and chemical (p, T, Gibbs) equilibrium Newton, one thread per cell.
+// Restates DP/relaxation.cu:4-75, DP/thermRlx.cu:4-235, DP/chemRlx.cu:4-267 on the device;
+// the partition is decided per cell in the same kernel instead of atomic-append lists
+// (cells are independent, so the result is identical and deterministic).
+// Every Newton loop is bounded by the reference's iteration caps (thermItrMax, chemItrMax,
+// 50 for the saturation temperature, urf > 0.0005 for step halving).
+#include "fg_kernels.cuh"
+
+namespace fg {
+
+namespace {
+
+struct Ph {
+    double g, pinf, cp, eta;
+};
+
+__device__ __forceinline__ double p_of(const Ph &h, double r, double e) {
+    return (h.g - 1) * r * e - h.g * h.pinf - (h.g - 1) * h.eta * r;
+}
+__device__ __forceinline__ double t_of(const Ph &h, double r, double e) {
+    const double p = (h.g - 1) * r * e - h.g * h.pinf - (h.g - 1) * h.eta * r;
+    return (p + h.pinf) / ((h.cp / h.g) * (h.g - 1) * r);
+}
+
+__device__ double sat_temp(const RelaxParams &R, double P, double temp, double urf) {
+    const double Pinf = R.pinf[0];
+    const double g1 = R.gam[0], g2 = R.gam[1];
+    const double Cp1 = R.cp[0], Cp2 = R.cp[1];
+    const double Cv1 = Cp1 / g1, Cv2 = Cp2 / g2;
+    const double etaT2 = R.satConst[0] * log10(P) + R.satConst[1];
+    const double As = (Cp1 - Cp2 + etaT2 - 0.0) / (Cp2 - Cv2);
+    const double Bs = (R.eta[0] - R.eta[1]) / (Cp2 - Cv2);
+    const double Cs = (Cp2 - Cp1) / (Cp2 - Cv2);
+    const double Ds = (Cp1 - Cv1) / (Cp2 - Cv2);
+    const double dT = 1.e-3;
+    const double lpp = Ds * log10(P + Pinf), lp = log10(P);
+    double fun = 1, T = temp;
+    for (int itr = 0; fabs(fun) > 1.e-2 && itr < 50; itr++) {
+        fun = As + Bs / T + Cs * log10(T) + lpp - lp;
+        const double fdt = As + Bs / (T + dT) + Cs * log10(T + dT) + lpp - lp;
+        T = T - urf * fun / ((fdt - fun) / dT);
+    }
+    return T;
+}
+
+__device__ __forceinline__ void therm_res(const Ph *h, int pm, double *x, const double *ar, const double *enr,
+                                          double *r0, double *r1) {
+    const int mm = 1 - pm;
+    const double s1 = ar[mm] / x[mm];
+    const double s2 = ar[mm] * (x[2 + mm] - enr[mm]);
+    x[pm] = (1 / (1 - s1)) * ar[pm];
+    x[2 + pm] = enr[pm] - (1 / ar[pm]) * s2;
+    *r0 = p_of(h[0], x[0], x[2]) - p_of(h[1], x[1], x[3]);
+    *r1 = t_of(h[0], x[0], x[2]) - t_of(h[1], x[1], x[3]);
+}
+
+__device__ int therm_cell(const RelaxParams &R, const Ph *h, double *U) {
+    double ar[2], enr[2], x[4], ax[4];
+    const double a0 = fmin(fmax(R.avfMin / 100, U[0]), 1 - R.avfMin / 100);
+    const double a1 = 1 - a0;
+    const double rho0 = U[1] / a0, rho1 = U[2] / a1;
+    ar[0] = a0 * rho0;
+    ar[1] = a1 * rho1;
+    enr[0] = U[6] / ar[0];
+    enr[1] = U[7] / ar[1];
+    const double rm = ar[0] + ar[1];
+    const double u = U[3] / rm, v = U[4] / rm, w = U[5] / rm;
+    x[0] = rho0; x[1] = rho1; x[2] = enr[0]; x[3] = enr[1];
+#pragma unroll
+    for (int i = 0; i < 4; i++) ax[i] = x[i];
+    const int pm = (a1 > a0) ? 1 : 0;
+    const double de = U[8] / rm - (ar[0] / rm) * enr[0] - (ar[1] / rm) * enr[1] - 0.5 * (u * u + v * v + w * w);
+    enr[0] += de;
+    enr[1] += de;
+    const int mm = 1 - pm;
+    float minRes = 1e9f;
+    int abortFlag = 0, aborted = 0;
+    for (int itr = 1;; itr++) {
+        double res[2], rdf[2][2], e[2];
+        therm_res(h, pm, x, ar, enr, &res[0], &res[1]);
+        // finite-difference Jacobian over the minor phase's (rho, e)
+        const int js[2] = {mm, mm + 2};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int j = js[q];
+            e[q] = 1e-4 * x[j];
+            x[j] += e[q];
+            therm_res(h, pm, x, ar, enr, &rdf[0][q], &rdf[1][q]);
+            x[j] -= e[q];
+        }
+        double jac[2][2];
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                jac[i][j] = (rdf[i][j] - res[i]) / e[j];
+                if (isnan(jac[i][j])) abortFlag = 1;
+            }
+        const double det = jac[0][0] * jac[1][1] - jac[1][0] * jac[0][1];
+        const double i00 = jac[1][1] / det, i11 = jac[0][0] / det, i10 = -jac[1][0] / det, i01 = -jac[0][1] / det;
+        if (det == 0) abortFlag = 1;
+        if (abortFlag == 0 && x[0] > 0.0 && x[1] > 0.0) {
+            const float chk = sqrt(res[0] * res[0] + res[1] * res[1]);
+            if (chk < minRes) {
+                minRes = chk;
+#pragma unroll
+                for (int i = 0; i < 4; i++) ax[i] = x[i];
+            }
+        }
+        x[mm] = x[mm] - R.thermUrf * (i00 * res[0] + i01 * res[1]);
+        x[mm + 2] = x[mm + 2] - R.thermUrf * (i10 * res[0] + i11 * res[1]);
+        const bool conv = !(fabs(res[0]) > 1.e-2) && !(fabs(res[1]) > 1.e-2);
+        if (abortFlag == 1 || itr > R.thermItrMax) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) x[i] = ax[i];
+            aborted = 1;
+            break;
+        }
+        if (conv) break;
+    }
+    const double s1 = ar[mm] / x[mm];
+    const double s2 = ar[mm] * (x[2 + mm] - enr[mm]);
+    x[pm] = (1 / (1 - s1)) * ar[pm];
+    x[2 + pm] = enr[pm] - (1 / ar[pm]) * s2;
+    U[0] = fmin(fmax(R.avfMin / 100, ar[0] / x[0]), 1 - R.avfMin / 100);
+    U[6] = ar[0] * x[2];
+    U[7] = ar[1] * x[3];
+    return aborted;
+}
+
+__device__ __forceinline__ double gibbs_of(const RelaxParams &R, int m, double P, double T) {
+    const double et = (m == 1) ? R.satConst[0] * log10(P) + R.satConst[1] : 0.0;
+    const double hh = R.cp[m] * T + R.eta[m];
+    const double s = (R.cp[m] / R.gam[m]) * log10(pow(T, R.gam[m]) / pow(P + R.pinf[m], R.gam[m] - 1)) + et;
+    return hh - T * s;
+}
+
+__device__ void chem_res(const RelaxParams &R, const Ph *h, int pm, double *x, double rm, double re, double *r) {
+    const int mm = 1 - pm;
+    const double s1 = x[mm], s2 = x[mm] * x[mm + 2], s3 = x[mm] * x[mm + 2] * x[mm + 4];
+    x[pm] = 1 - s1;
+    x[pm + 2] = (rm - s2) / x[pm];
+    x[pm + 4] = (re - s3) / (x[pm] * x[pm + 2]);
+    double p[2], T[2];
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+        p[m] = p_of(h[m], x[m + 2], x[m + 4]);
+        T[m] = t_of(h[m], x[m + 2], x[m + 4]);
+    }
+    r[0] = p[0] - p[1];
+    r[1] = T[0] - T[1];
+    r[2] = gibbs_of(R, 0, p[0], T[0]) - gibbs_of(R, 1, p[1], T[1]);
+}
+
+__device__ void chem_check(const RelaxParams &R, double xOld, double *x, double dx, int i, float urf, int *ab, double rho) {
+    if (i == 0 || i == 1) {
+        if (x[i] < 0) { while (x[i] < R.chemLimit && urf > 0.0005f) { urf = urf / 2; x[i] = xOld - urf * dx; } }
+        if (x[i] > 1) { while (x[i] > 1.0 - R.chemLimit && urf > 0.0005f) { urf = urf / 2; x[i] = xOld - urf * dx; } }
+        if (x[i] < 0) *ab = 1;
+        if (x[i] > 1) *ab = 1;
+    } else if (i == 2 || i == 3) {
+        double ar = x[i - 2] * x[i];
+        if (x[i] < 0) { while (x[i] < 0 && urf > 0.0005f) { urf = urf / 2; x[i] = xOld - urf * dx; } }
+        if (ar > rho) { while (ar > rho && urf > 0.0005f) { urf = urf / 2; x[i] = xOld - urf * dx; ar = x[i - 2] * x[i]; } }
+        if (x[i] < 0) *ab = 1;
+        if (ar > rho) *ab = 1;
+    }
+}
+
+__device__ int chem_cell(const RelaxParams &R, const Ph *h, double *U) {
+    double x[6], ax[6];
+    x[0] = fmin(fmax(R.avfMin / 100, U[0]), 1 - R.avfMin / 100);
+    x[1] = 1 - x[0];
+    x[2] = U[1] / x[0];
+    x[3] = U[2] / x[1];
+    x[4] = U[6] / (x[0] * x[2]);
+    x[5] = U[7] / (x[1] * x[3]);
+#pragma unroll
+    for (int i = 0; i < 6; i++) ax[i] = x[i];
+    const double rm = x[0] * x[2] + x[1] * x[3];
+    const double u = U[3] / rm, v = U[4] / rm, w = U[5] / rm;
+    const double re = U[8] - 0.5 * rm * (u * u + v * v + w * w);
+    const int pm = (x[1] > x[0]) ? 1 : 0;
+    const int mm = 1 - pm;
+    float minRes = 1e9f;
+    int abortFlag = 0, aborted = 0;
+    for (int itr = 1;; itr++) {
+        double res[3], rdf[3][3], e[3];
+        chem_res(R, h, pm, x, rm, re, res);
+        const int js[3] = {mm, mm + 2, mm + 4};
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const int j = js[q];
+            e[q] = fabs(x[j]) < 1e-9 ? 1e-10 : 1.e-5 * x[j];
+            x[j] += e[q];
+            double rr[3];
+            chem_res(R, h, pm, x, rm, re, rr);
+            rdf[0][q] = rr[0]; rdf[1][q] = rr[1]; rdf[2][q] = rr[2];
+            x[j] -= e[q];
+        }
+        double j_[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                j_[i][j] = (rdf[i][j] - res[i]) / e[j];
+                if (isnan(j_[i][j])) abortFlag = 1;
+            }
+        const double det = j_[0][0] * (j_[1][1] * j_[2][2] - j_[1][2] * j_[2][1]) -
+                           j_[0][1] * (j_[1][0] * j_[2][2] - j_[1][2] * j_[2][0]) +
+                           j_[0][2] * (j_[1][0] * j_[2][1] - j_[1][1] * j_[2][0]);
+        if (det == 0) abortFlag = 1;
+        const double id = 1.0 / det;
+        double inv[3][3];
+        inv[0][0] = id * (j_[1][1] * j_[2][2] - j_[1][2] * j_[2][1]);
+        inv[0][1] = -id * (j_[0][1] * j_[2][2] - j_[0][2] * j_[2][1]);
+        inv[0][2] = id * (j_[0][1] * j_[1][2] - j_[0][2] * j_[1][1]);
+        inv[1][0] = -id * (j_[1][0] * j_[2][2] - j_[1][2] * j_[2][0]);
+        inv[1][1] = id * (j_[0][0] * j_[2][2] - j_[0][2] * j_[2][0]);
+        inv[1][2] = -id * (j_[0][0] * j_[1][2] - j_[0][2] * j_[1][0]);
+        inv[2][0] = id * (j_[1][0] * j_[2][1] - j_[1][1] * j_[2][0]);
+        inv[2][1] = -id * (j_[0][0] * j_[2][1] - j_[0][1] * j_[2][0]);
+        inv[2][2] = id * (j_[0][0] * j_[1][1] - j_[0][1] * j_[1][0]);
+        if (abortFlag == 0 && x[0] > 0.0 && x[0] < 1.0 && x[1] > 0.0 && x[1] < 1.0 && x[2] > 0.0 && x[3] > 0.0) {
+            const float chk = sqrt(res[0] * res[0] + res[1] * res[1] + res[2] * res[2]);
+            if (chk < minRes) {
+                minRes = chk;
+#pragma unroll
+                for (int i = 0; i < 6; i++) ax[i] = x[i];
+            }
+        }
+        int abLocal = abortFlag;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const int i = js[q];
+            const double dx = inv[q][0] * res[0] + inv[q][1] * res[1] + inv[q][2] * res[2];
+            x[i] = x[i] - R.chemUrf * dx;
+            chem_check(R, x[i] + R.chemUrf * dx, x, dx, i, (float)R.chemUrf, &abLocal, rm);
+        }
+        const bool conv = !(fabs(res[0]) > 1.e-1) && !(fabs(res[1]) > 1.e-1) && !(fabs(res[2]) > 1.e-1);
+        if (abLocal == 1 || itr > R.chemItrMax) {
+#pragma unroll
+            for (int i = 0; i < 6; i++) x[i] = ax[i];
+            aborted = 1;
+            break;
+        }
+        if (conv) break;
+    }
+    const double s1 = x[mm], s2 = x[mm] * x[mm + 2], s3 = x[mm] * x[mm + 2] * x[mm + 4];
+    x[pm] = 1 - s1;
+    x[pm + 2] = (rm - s2) / x[pm];
+    x[pm + 4] = (re - s3) / (x[pm] * x[pm + 2]);
+    U[0] = fmin(fmax(R.avfMin / 100, x[0]), 1 - R.avfMin / 100);
+    U[1] = x[0] * x[2];
+    U[2] = x[1] * x[3];
+    U[6] = x[0] * x[2] * x[4];
+    U[7] = x[1] * x[3] * x[5];
+    U[9] = x[1] * x[3];
+    return aborted;
+}
+
+}  // namespace
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R, int32_t *counters) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int chem = 0, ab = 0;
+    const bool act = c < n;
+    if (act) {
+        double u[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
+        const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
+        if (R.chemFlag == 1) {
+            const double avf = fmin(fmax(R.avfMin / 100, u[0]), 1 - R.avfMin / 100);
+            const double rho = u[1] / avf;
+            const double enr = u[6] / (avf * rho);
+            const double tl = t_of(h[0], rho, enr);
+            const double pl = p_of(h[0], rho, enr);
+            const double ts = sat_temp(R, pl, tl, R.satTempUrf);
+            chem = (tl > ts && avf > R.chemLimit);
+        }
+        ab = chem ? chem_cell(R, h, u) : therm_cell(R, h, u);
+        U[(size_t)0 * n + c] = u[0];
+        U[(size_t)1 * n + c] = u[1];
+        U[(size_t)2 * n + c] = u[2];
+        U[(size_t)6 * n + c] = u[6];
+        U[(size_t)7 * n + c] = u[7];
+        U[(size_t)9 * n + c] = u[9];
+        T w[NP];
+        cons2prim_d(D, u, w);
+        T *p = W + (size_t)c * WREC;
+#pragma unroll
+        for (int v = 0; v < NP; v++) p[v] = w[v];
+#pragma unroll
+        for (int v = NP; v < WREC; v++) p[v] = 0;
+    }
+    // warp-aggregated counters (counts only: order does not matter)
+    const unsigned mask = __ballot_sync(0xffffffffu, act && chem);
+    const unsigned maskT = __ballot_sync(0xffffffffu, act && !chem);
+    const unsigned maskA = __ballot_sync(0xffffffffu, act && ab);
+    if ((threadIdx.x & 31) == 0) {
+        if (maskT) atomicAdd(&counters[0], __popc(maskT));
+        if (mask) atomicAdd(&counters[1], __popc(mask));
+        if (maskA) atomicAdd(&counters[2], __popc(maskA));
+    }
+}
+
+template <typename T>
+void launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters, cudaStream_t s) {
+    k_relax<T><<<(n + 127) / 128, 128, 0, s>>>(n, U, W, D, R, counters);
+}
+
+template void launch_relax<float>(int, double *, float *, const PhysD &, const RelaxParams &, int32_t *, cudaStream_t);
+template void launch_relax<double>(int, double *, double *, const PhysD &, const RelaxParams &, int32_t *, cudaStream_t);
+
+}  // namespace fg

@@ -1,0 +1,740 @@
+// C ABI of the device residual path: solver lifetime, state transfer, stage functions and the
+// explicitLoop step (host side).  See include/fooskagpu.h for the reference function each
+// entry point replaces.
+#include "../../include/fooskagpu.h"
+#include "fg_kernels.cuh"
+#include "fg_mesh.h"
+
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err = "";
+
+int set_err(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define FG_CUDA_TRY(expr)                                                                         \
+    do {                                                                                          \
+        cudaError_t e_ = (expr);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return set_err(e_ == cudaErrorMemoryAllocation ? FG_ERR_NOMEM : FG_ERR_CUDA,          \
+                           std::string(#expr) + ": " + cudaGetErrorString(e_));                   \
+    } while (0)
+
+#define FG_LAUNCH_CHECK(what)                                                                     \
+    do {                                                                                          \
+        cudaError_t e_ = cudaGetLastError();                                                      \
+        if (e_ != cudaSuccess) return set_err(FG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t b) {
+        bytes = b;
+        return cudaMalloc(&p, b ? b : 16);
+    }
+    template <typename X>
+    X *as() const { return reinterpret_cast<X *>(p); }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------ solver base
+struct fg_solver {
+    virtual ~fg_solver() {
+        for (cudaEvent_t e : evPool) cudaEventDestroy(e);
+    }
+    int device = 0;
+    // ---- instrumentation: events around every launch when enabled
+    bool prof = false;
+    std::vector<cudaEvent_t> evPool;
+    size_t evUsed = 0;
+    std::vector<int> recKind;
+    uint64_t launches = 0;
+    cudaEvent_t ev_next() {
+        if (evUsed == evPool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            evPool.push_back(e);
+        }
+        return evPool[evUsed++];
+    }
+    void prof_begin(int kind, cudaStream_t s) {
+        launches++;
+        if (!prof) return;
+        recKind.push_back(kind);
+        cudaEventRecord(ev_next(), s);
+    }
+    void prof_end(cudaStream_t s) {
+        if (!prof) return;
+        cudaEventRecord(ev_next(), s);
+    }
+    int prof_read(fg_kernel_times *out) {
+        memset(out, 0, sizeof(*out));
+        if (cudaDeviceSynchronize() != cudaSuccess) return set_err(FG_ERR_CUDA, "profile read: device error");
+        for (size_t i = 0; i < recKind.size(); i++) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, evPool[2 * i], evPool[2 * i + 1]);
+            out->ms[recKind[i]] += ms;
+            out->launches[recKind[i]]++;
+        }
+        return FG_OK;
+    }
+    void prof_reset(bool en) {
+        prof = en;
+        evUsed = 0;
+        recKind.clear();
+    }
+    fg_case cs{};
+    int n = 0, nSlots = 0;
+    int iStep = 0;
+    uint64_t bytes = 0;
+    virtual int init(const fg::Mesh &m) = 0;
+    virtual int set_state(const double *U, cudaStream_t s) = 0;
+    virtual int get_state(double *U, cudaStream_t s) = 0;
+    virtual int compute_rhs(int wantSignal, cudaStream_t s) = 0;
+    virtual int time_step(double *dtOut, cudaStream_t s) = 0;
+    virtual int init_rk(cudaStream_t s) = 0;
+    virtual int update(int irk, int writeU0, cudaStream_t s) = 0;
+    virtual int stage(int irk, int writeU0, cudaStream_t s) = 0;
+    virtual int relax(fg_relax_stats *st, cudaStream_t s) = 0;
+    virtual int cons(int ivar, double *out, cudaStream_t s) = 0;
+    virtual int advance_time(cudaStream_t s) = 0;
+    virtual int get_time(double *dt, double *t) = 0;
+    virtual int set_dt(double dt) = 0;
+    virtual int get_rhs(double *rhs) = 0;
+    virtual int get_limited(double *grad, double *theta) = 0;
+    virtual int get_signal(double *sig) = 0;
+};
+
+namespace fg {
+
+__global__ void k_advance_time(const double *dt, double *t) { *t += *dt; }
+
+template <typename T>
+struct SolverT : public fg_solver {
+    DevBuf dNbr, dFlags, dGeo, dVol, dVolP, dNew2Old;
+    DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dBlockMin, dScal, dCnt, dCons, dStage;
+    int cur = 0;
+    DevMesh<T> dm{};
+    PhysT<T> P{};
+    PhysD D{};
+    RelaxParams R{};
+
+    Fields<T> fields(int wIn) {
+        Fields<T> f;
+        f.U = dU.as<double>();
+        f.U0 = dU0.as<double>();
+        f.RHS = dRHS.as<double>();
+        f.Win = dW[wIn].as<T>();
+        f.Wout = dW[1 - wIn].as<T>();
+        f.G = dG.as<T>();
+        f.signal = dSig.as<double>();
+        f.blockMin = dBlockMin.as<double>();
+        f.dt = dScal.as<double>();
+        return f;
+    }
+
+    int init(const fg::Mesh &m) override {
+        n = m.nElem;
+        nSlots = m.maxFaces;
+        // physics constants in T and FP64
+        for (int k = 0; k < 2; k++) {
+            const double g = cs.gamma[k];
+            P.gam[k] = (T)g;
+            P.gm1[k] = (T)(g - 1);
+            P.gp1[k] = (T)(g + 1);
+            P.pinf[k] = (T)cs.pInf[k];
+            P.gpinf[k] = (T)(g * cs.pInf[k]);
+            P.cvgm1[k] = (T)((cs.Cp[k] / g) * (g - 1));
+            P.gm1eta[k] = (T)((g - 1) * cs.eta[k]);
+            P.mu[k] = (T)cs.dynVisc[k];
+            D.gam[k] = g;
+            D.gm1[k] = g - 1;
+            D.pinf[k] = cs.pInf[k];
+            D.gpinf[k] = g * cs.pInf[k];
+            D.cvgm1[k] = (cs.Cp[k] / g) * (g - 1);
+            D.gm1eta[k] = (g - 1) * cs.eta[k];
+            R.gam[k] = g;
+            R.pinf[k] = cs.pInf[k];
+            R.cp[k] = cs.Cp[k];
+            R.eta[k] = cs.eta[k];
+            R.satConst[k] = cs.satConst[k];
+        }
+        D.avfLo = cs.avfMin / 100;
+        D.avfHi = 1.0 - cs.avfMin / 100;
+        P.chemLimit = (T)cs.chemLimit;
+        P.woods = (cs.woodsFlag == 1);
+        P.visc = (cs.viscFlag == 1);
+        P.turb = (cs.turbulence == 1);
+        {
+            // inlet ghost (DP/bc.h:2-25): rho from p = 11.4e5 Pa, T = 115.3 K
+            const double pIn = 11.4e5, tIn = 115.3;
+            P.inAlpha = (T)(1.0 - cs.avfMin);
+            P.inRhoL = (T)((pIn + cs.pInf[0]) / ((cs.Cp[0] / cs.gamma[0]) * tIn * (cs.gamma[0] - 1)));
+            P.inRhoG = (T)((pIn + cs.pInf[1]) / ((cs.Cp[1] / cs.gamma[1]) * tIn * (cs.gamma[1] - 1)));
+            P.inP = (T)pIn;
+        }
+        R.avfMin = cs.avfMin;
+        R.chemLimit = cs.chemLimit;
+        R.thermUrf = cs.thermUrf;
+        R.chemUrf = cs.chemUrf;
+        R.satTempUrf = cs.satTempUrf;
+        R.thermItrMax = cs.thermItrMax;
+        R.chemItrMax = cs.chemItrMax;
+        R.chemFlag = cs.chemFlag;
+
+        // ---- device mesh (ELL slots in element-local face order) ----
+        const int nF = m.nFcs;
+        std::vector<int32_t> elFc2fc((size_t)m.nElem * 6, -1), elFcSide((size_t)m.nElem * 6, 0);
+        for (int f = 0; f < nF; f++) {
+            elFc2fc[(size_t)m.fc2el[2 * f] * 6 + m.fc2elFc[2 * f]] = f;
+            elFcSide[(size_t)m.fc2el[2 * f] * 6 + m.fc2elFc[2 * f]] = 0;
+            if (m.boundCond[f] == 0) {
+                elFc2fc[(size_t)m.fc2el[2 * f + 1] * 6 + m.fc2elFc[2 * f + 1]] = f;
+                elFcSide[(size_t)m.fc2el[2 * f + 1] * 6 + m.fc2elFc[2 * f + 1]] = 1;
+            }
+        }
+        const size_t S = (size_t)nSlots * n;
+        std::vector<int32_t> nbr(S, INT32_MIN), flags(n, 0);
+        std::vector<T> geo(10 * S, (T)0);
+        std::vector<double> volP(n), vol(n);
+        for (int i = 0; i < n; i++) {
+            const int o = m.new2old[i];
+            const fg::ElemType *et = fg::elem_type_for_nodes(m.elNN[o]);
+            int fl = et->nFaces;
+            vol[i] = m.volume[o];
+            volP[i] = pow(m.volume[o], 0.3333);
+            for (int k = 0; k < et->nFaces; k++) {
+                const int f = elFc2fc[(size_t)o * 6 + k];
+                const int side = elFcSide[(size_t)o * 6 + k];
+                if (f < 0) return set_err(FG_ERR_MESH, "internal: element face without a face record");
+                const size_t q = (size_t)k * n + i;
+                const int bc = m.boundCond[f];
+                const int own = m.fc2el[2 * f], nbo = m.fc2el[2 * f + 1];
+                const double *fc = &m.fcCenter[(size_t)f * 3];
+                const double *sh = &m.nbShift[(size_t)f * 3];
+                double xOwnSide[3], xNbSide[3];
+                for (int d = 0; d < 3; d++) {
+                    xOwnSide[d] = fc[d];
+                    xNbSide[d] = fc[d] + sh[d];
+                }
+                if (side == 0) {
+                    fl |= 1 << (3 + k);
+                    nbr[q] = (bc == 0) ? m.old2new[nbo] : -bc;
+                } else {
+                    nbr[q] = m.old2new[own];
+                }
+                for (int d = 0; d < 3; d++) geo[(size_t)d * S + q] = (T)m.n[(size_t)f * 3 + d];
+                geo[3 * S + q] = (T)m.area[f];
+                for (int d = 0; d < 3; d++) {
+                    const double dcv = (side == 0) ? xOwnSide[d] - m.cellCenter[(size_t)o * 3 + d]
+                                                   : xNbSide[d] - m.cellCenter[(size_t)o * 3 + d];
+                    double dnv = 0.0;
+                    if (side == 0 && bc == 0) dnv = xNbSide[d] - m.cellCenter[(size_t)nbo * 3 + d];
+                    if (side == 1) dnv = xOwnSide[d] - m.cellCenter[(size_t)own * 3 + d];
+                    geo[(size_t)(4 + d) * S + q] = (T)dcv;
+                    geo[(size_t)(7 + d) * S + q] = (T)dnv;
+                }
+            }
+            flags[i] = fl;
+        }
+        FG_CUDA_TRY(cudaSetDevice(device));
+        FG_CUDA_TRY(dNbr.alloc(S * sizeof(int32_t)));
+        FG_CUDA_TRY(dFlags.alloc((size_t)n * sizeof(int32_t)));
+        FG_CUDA_TRY(dGeo.alloc(10 * S * sizeof(T)));
+        FG_CUDA_TRY(dVol.alloc((size_t)n * sizeof(double)));
+        FG_CUDA_TRY(dVolP.alloc((size_t)n * sizeof(double)));
+        FG_CUDA_TRY(dNew2Old.alloc((size_t)n * sizeof(int32_t)));
+        FG_CUDA_TRY(cudaMemcpy(dNbr.p, nbr.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dFlags.p, flags.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dGeo.p, geo.data(), 10 * S * sizeof(T), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dVol.p, vol.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dVolP.p, volP.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dNew2Old.p, m.new2old.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        const size_t u = (size_t)n * NV * sizeof(double);
+        FG_CUDA_TRY(dU.alloc(u));
+        FG_CUDA_TRY(dU0.alloc(u));
+        FG_CUDA_TRY(dRHS.alloc(u));
+        FG_CUDA_TRY(dStage.alloc(u));
+        FG_CUDA_TRY(dW[0].alloc((size_t)n * WREC * sizeof(T)));
+        FG_CUDA_TRY(dW[1].alloc((size_t)n * WREC * sizeof(T)));
+        FG_CUDA_TRY(dG.alloc((size_t)n * GREC * sizeof(T)));
+        FG_CUDA_TRY(dSig.alloc((size_t)n * sizeof(double)));
+        FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n), cons_blocks(n)) * sizeof(double)));
+        FG_CUDA_TRY(dScal.alloc(4 * sizeof(double)));   // dt, time, cons
+        FG_CUDA_TRY(dCnt.alloc(4 * sizeof(int32_t)));
+        FG_CUDA_TRY(cudaMemset(dU.p, 0, u));
+        FG_CUDA_TRY(cudaMemset(dU0.p, 0, u));
+        FG_CUDA_TRY(cudaMemset(dRHS.p, 0, u));
+        FG_CUDA_TRY(cudaMemset(dW[0].p, 0, (size_t)n * WREC * sizeof(T)));
+        FG_CUDA_TRY(cudaMemset(dW[1].p, 0, (size_t)n * WREC * sizeof(T)));
+        FG_CUDA_TRY(cudaMemset(dG.p, 0, (size_t)n * GREC * sizeof(T)));
+        const double scal[4] = {cs.dt, 0.0, 0.0, 0.0};
+        FG_CUDA_TRY(cudaMemcpy(dScal.p, scal, sizeof(scal), cudaMemcpyHostToDevice));
+        bytes = 0;
+        for (DevBuf *b : {&dNbr, &dFlags, &dGeo, &dVol, &dVolP, &dNew2Old, &dU, &dU0, &dRHS, &dStage, &dW[0], &dW[1], &dG,
+                          &dSig, &dBlockMin, &dScal, &dCnt})
+            bytes += b->bytes;
+        dm.n = n;
+        dm.nSlots = nSlots;
+        dm.nbr = dNbr.as<int32_t>();
+        dm.flags = dFlags.as<int32_t>();
+        T *g = dGeo.as<T>();
+        dm.nx = g + 0 * S; dm.ny = g + 1 * S; dm.nz = g + 2 * S; dm.A = g + 3 * S;
+        dm.dcx = g + 4 * S; dm.dcy = g + 5 * S; dm.dcz = g + 6 * S;
+        dm.dnx = g + 7 * S; dm.dny = g + 8 * S; dm.dnz = g + 9 * S;
+        dm.vol = dVol.as<double>();
+        dm.volP = dVolP.as<double>();
+        return FG_OK;
+    }
+
+    int set_state(const double *U, cudaStream_t s) override {
+        FG_CUDA_TRY(cudaMemcpyAsync(dStage.p, U, (size_t)n * NV * sizeof(double), cudaMemcpyHostToDevice, s));
+        prof_begin(FG_K_OTHER, s);
+        launch_scatter_state(n, dStage.as<double>(), dNew2Old.as<int32_t>(), dU.as<double>(), s);
+        prof_end(s);
+        prof_begin(FG_K_OTHER, s);
+        launch_prim<T>(n, dU.as<double>(), dW[cur].as<T>(), D, s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("set_state");
+        return FG_OK;
+    }
+    int get_state(double *U, cudaStream_t s) override {
+        prof_begin(FG_K_OTHER, s);
+        launch_gather_state(n, dU.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("get_state");
+        FG_CUDA_TRY(cudaMemcpyAsync(U, dStage.p, (size_t)n * NV * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FG_CUDA_TRY(cudaStreamSynchronize(s));
+        return FG_OK;
+    }
+    StageCoef coef(int irk, int writeU0) const {
+        StageCoef sc;
+        sc.rk = (cs.rkSteps == 3) ? 3 : 1;
+        sc.irk = irk;
+        sc.writeU0 = writeU0;
+        sc.neglectZ = (cs.neglectZ == 1);
+        return sc;
+    }
+    int compute_rhs(int wantSignal, cudaStream_t s) override {
+        Fields<T> f = fields(cur);
+        prof_begin(FG_K_GRAD, s);
+        launch_grad<T>(dm, f, P, s);
+        prof_end(s);
+        prof_begin(FG_K_FLUX, s);
+        launch_flux<T>(dm, f, P, D, FLUX_RHS, wantSignal, coef(0, 0), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("compute_rhs");
+        return FG_OK;
+    }
+    int time_step(double *dtOut, cudaStream_t s) override {
+        prof_begin(FG_K_DT, s);
+        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(n), cs.cfl, cs.maxDt, dScal.as<double>(), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("time_step");
+        if (dtOut) {
+            FG_CUDA_TRY(cudaMemcpyAsync(dtOut, dScal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+            FG_CUDA_TRY(cudaStreamSynchronize(s));
+        }
+        return FG_OK;
+    }
+    int init_rk(cudaStream_t s) override {
+        prof_begin(FG_K_OTHER, s);
+        launch_copy_u0(n, dU.as<double>(), dU0.as<double>(), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("init_rk");
+        return FG_OK;
+    }
+    int update(int irk, int writeU0, cudaStream_t s) override {
+        Fields<T> f = fields(cur);
+        prof_begin(FG_K_UPDATE, s);
+        launch_update<T>(dm, f, D, coef(irk, writeU0), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("update");
+        cur ^= 1;
+        return FG_OK;
+    }
+    int stage(int irk, int writeU0, cudaStream_t s) override {
+        Fields<T> f = fields(cur);
+        prof_begin(FG_K_GRAD, s);
+        launch_grad<T>(dm, f, P, s);
+        prof_end(s);
+        prof_begin(FG_K_FLUX, s);
+        launch_flux<T>(dm, f, P, D, FLUX_FUSED, 0, coef(irk, writeU0), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("stage");
+        cur ^= 1;
+        return FG_OK;
+    }
+    int relax(fg_relax_stats *st, cudaStream_t s) override {
+        FG_CUDA_TRY(cudaMemsetAsync(dCnt.p, 0, 4 * sizeof(int32_t), s));
+        prof_begin(FG_K_RELAX, s);
+        launch_relax<T>(n, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("relaxation");
+        if (st) {
+            int32_t h[4];
+            FG_CUDA_TRY(cudaMemcpyAsync(h, dCnt.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+            FG_CUDA_TRY(cudaStreamSynchronize(s));
+            st->nTherm = h[0];
+            st->nChem = h[1];
+            st->nAbort = h[2];
+            st->reserved = 0;
+        }
+        return FG_OK;
+    }
+    int cons(int ivar, double *out, cudaStream_t s) override {
+        double *o = dScal.as<double>() + 2;
+        prof_begin(FG_K_CONS, s);
+        launch_cons(n, ivar, dU.as<double>(), dVol.as<double>(), dBlockMin.as<double>(), o, s);
+        prof_end(s);
+        launches++;  // two kernels
+        FG_LAUNCH_CHECK("cons_calc");
+        if (out) {
+            FG_CUDA_TRY(cudaMemcpyAsync(out, o, sizeof(double), cudaMemcpyDeviceToHost, s));
+            FG_CUDA_TRY(cudaStreamSynchronize(s));
+        }
+        return FG_OK;
+    }
+    int advance_time(cudaStream_t s) override {
+        prof_begin(FG_K_OTHER, s);
+        k_advance_time<<<1, 1, 0, s>>>(dScal.as<double>(), dScal.as<double>() + 1);
+        prof_end(s);
+        FG_LAUNCH_CHECK("advance_time");
+        return FG_OK;
+    }
+    int get_time(double *dt, double *t) override {
+        double h[2];
+        FG_CUDA_TRY(cudaDeviceSynchronize());
+        FG_CUDA_TRY(cudaMemcpy(h, dScal.p, sizeof(h), cudaMemcpyDeviceToHost));
+        if (dt) *dt = h[0];
+        if (t) *t = h[1];
+        return FG_OK;
+    }
+    int set_dt(double dt) override {
+        FG_CUDA_TRY(cudaDeviceSynchronize());
+        FG_CUDA_TRY(cudaMemcpy(dScal.p, &dt, sizeof(double), cudaMemcpyHostToDevice));
+        return FG_OK;
+    }
+    int get_rhs(double *rhs) override {
+        launch_gather_state(n, dRHS.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), 0);
+        FG_LAUNCH_CHECK("get_rhs");
+        FG_CUDA_TRY(cudaMemcpy(rhs, dStage.p, (size_t)n * NV * sizeof(double), cudaMemcpyDeviceToHost));
+        return FG_OK;
+    }
+    int get_limited(double *grad, double *theta) override {
+        FG_CUDA_TRY(cudaDeviceSynchronize());
+        std::vector<T> g((size_t)n * GREC);
+        std::vector<int32_t> n2o(n);
+        FG_CUDA_TRY(cudaMemcpy(g.data(), dG.p, g.size() * sizeof(T), cudaMemcpyDeviceToHost));
+        FG_CUDA_TRY(cudaMemcpy(n2o.data(), dNew2Old.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; i++) {
+            const size_t o = (size_t)n2o[i];
+            for (int v = 0; v < NV; v++) {
+                if (theta) theta[o * NV + v] = (v < NP) ? (double)g[(size_t)i * GREC + v] : 0.0;
+                for (int d = 0; d < 3; d++)
+                    if (grad) grad[(o * NV + v) * 3 + d] = (v < NP) ? (double)g[(size_t)i * GREC + NP + 3 * v + d] : 0.0;
+            }
+        }
+        return FG_OK;
+    }
+    int get_signal(double *sig) override {
+        FG_CUDA_TRY(cudaDeviceSynchronize());
+        std::vector<double> h(n);
+        std::vector<int32_t> n2o(n);
+        FG_CUDA_TRY(cudaMemcpy(h.data(), dSig.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+        FG_CUDA_TRY(cudaMemcpy(n2o.data(), dNew2Old.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; i++) sig[n2o[i]] = h[i];
+        return FG_OK;
+    }
+};
+
+}  // namespace fg
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char *fg_last_error(void) { return g_err.c_str(); }
+
+void fg_case_default(fg_case *c) {
+    // values hard-coded in DP/buildInput.cu:10-69
+    if (!c) return;
+    memset(c, 0, sizeof(*c));
+    c->dt = 0.0;
+    c->adaptDt = 1;
+    c->adaptDtItr = 100;
+    c->maxDt = 1e-8;
+    c->cfl = 0.1;
+    c->avfMin = 1e-4;
+    c->rkSteps = 1;
+    c->finalTime = 3.5e-3;
+    c->exportTime = 2.0e-5;
+    c->restartStep = 100000;
+    c->restartFlag = 0;
+    c->neglectX = 0;
+    c->neglectY = 0;
+    c->neglectZ = 0;
+    c->nMaterials = 2;
+    c->NEQ = 10;
+    c->scale = 0.001;
+    c->viscFlag = 1;
+    c->turbulence = 1;
+    c->woodsFlag = 1;
+    c->thermFntRlxFlag = 0;
+    c->thermRlxRate = 0.5;
+    c->thermUrf = 0.8;
+    c->thermItrMax = 25;
+    c->chemFlag = 1;
+    c->chemFntRlxFlag = 0;
+    c->chemRlxRate = 0;
+    c->chemUrf = 0.5;
+    c->chemItrMax = 40;
+    c->chemCondesation = 0;
+    c->chemLimit = 20e-4;
+    c->consCalcFlag = 1;
+    c->consCalcIvar = 9;
+    c->satTempUrf = 0.8;
+    c->gamma[0] = 2.17290;
+    c->pInf[0] = 114907765;
+    c->Cp[0] = 1854.4;
+    c->eta[0] = -302568.5557;
+    c->satConst[0] = -488.9933492;
+    c->dynVisc[0] = 1.8e-4;
+    c->gamma[1] = 1.4588;
+    c->pInf[1] = 0.0;
+    c->Cp[1] = 965.98;
+    c->eta[1] = 9741.04362;
+    c->satConst[1] = 297.63826;
+    c->dynVisc[1] = 1.99e-5;
+}
+
+int fg_mesh_load_neu(const char *path, const fg_mesh_opts *opts, fg_mesh **out) {
+    if (!path || !out) return set_err(FG_ERR_ARG, "fg_mesh_load_neu: null argument");
+    *out = nullptr;
+    fg_mesh_opts o{};
+    o.scale = 1.0;
+    o.renumber = FG_RENUMBER_MORTON;
+    if (opts) o = *opts;
+    if (!(o.scale > 0)) return set_err(FG_ERR_ARG, "fg_mesh_load_neu: scale must be > 0");
+    std::unique_ptr<fg_mesh> m(new fg_mesh());
+    std::string err;
+    int rc = fg::read_neu(path, o.scale, m->m, err);
+    if (rc != FG_OK) return set_err(rc, err);
+    rc = fg::finish_mesh(m->m, o, err);
+    if (rc != FG_OK) return set_err(rc, err);
+    *out = m.release();
+    return FG_OK;
+}
+
+int fg_mesh_info_get(const fg_mesh *mm, fg_mesh_info *info) {
+    if (!mm || !info) return set_err(FG_ERR_ARG, "fg_mesh_info_get: null argument");
+    const fg::Mesh &m = mm->m;
+    info->nElem = m.nElem;
+    info->nNodes = m.nNodes;
+    info->nFcs = m.nFcs;
+    info->nBoundary = m.nBoundary;
+    info->nPeriodic = m.nPeriodic;
+    info->maxFaces = m.maxFaces;
+    info->nTet = m.nTet;
+    info->nPyr = m.nPyr;
+    info->nPrism = m.nPrism;
+    info->nHex = m.nHex;
+    return FG_OK;
+}
+
+int fg_mesh_view_get(const fg_mesh *mm, fg_mesh_view *v) {
+    if (!mm || !v) return set_err(FG_ERR_ARG, "fg_mesh_view_get: null argument");
+    const fg::Mesh &m = mm->m;
+    v->nElem = m.nElem;
+    v->nFcs = m.nFcs;
+    v->fc2el = m.fc2el.data();
+    v->boundCond = m.boundCond.data();
+    v->cellCenter = m.cellCenter.data();
+    v->fcCenter = m.fcCenter.data();
+    v->n = m.n.data();
+    v->nt1 = m.nt1.data();
+    v->nt2 = m.nt2.data();
+    v->area = m.area.data();
+    v->volume = m.volume.data();
+    v->nbShift = m.nbShift.data();
+    return FG_OK;
+}
+
+int fg_mesh_permutation(const fg_mesh *mm, int32_t *new2old, int32_t n) {
+    if (!mm || !new2old) return set_err(FG_ERR_ARG, "fg_mesh_permutation: null argument");
+    if (n != mm->m.nElem) return set_err(FG_ERR_ARG, "fg_mesh_permutation: size mismatch");
+    memcpy(new2old, mm->m.new2old.data(), sizeof(int32_t) * (size_t)n);
+    return FG_OK;
+}
+
+void fg_mesh_free(fg_mesh *m) { delete m; }
+
+int fg_solver_create(const fg_mesh *m, const fg_case *c, int32_t precision, int32_t device, fg_solver **out) {
+    if (!m || !c || !out) return set_err(FG_ERR_ARG, "fg_solver_create: null argument");
+    *out = nullptr;
+    if (c->rkSteps != 1 && c->rkSteps != 3) return set_err(FG_ERR_UNSUPPORTED, "rkSteps must be 1 or 3");
+    if (c->thermFntRlxFlag != 0 || c->chemFntRlxFlag != 0)
+        return set_err(FG_ERR_UNSUPPORTED, "finite-rate relaxation (thermFntRlxFlag/chemFntRlxFlag) is not supported");
+    if (c->adaptDt == 1 && c->adaptDtItr <= 0) return set_err(FG_ERR_ARG, "adaptDtItr must be > 0");
+    if (m->m.maxFaces > fg::MAXSLOT) return set_err(FG_ERR_MESH, "cell with more than 6 faces");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_err(FG_ERR_CUDA, "no CUDA device available (the device path has no CPU fallback)");
+    if (device < 0 || device >= ndev) return set_err(FG_ERR_ARG, "device index out of range");
+    std::unique_ptr<fg_solver> s;
+    if (precision == FG_PREC_FP64) s.reset(new fg::SolverT<double>());
+    else if (precision == FG_PREC_MIXED) s.reset(new fg::SolverT<float>());
+    else return set_err(FG_ERR_ARG, "unknown precision");
+    s->device = device;
+    s->cs = *c;
+    int rc = s->init(m->m);
+    if (rc != FG_OK) return rc;
+    *out = s.release();
+    return FG_OK;
+}
+
+int fg_solver_destroy(fg_solver *s) {
+    if (!s) return FG_OK;
+    cudaSetDevice(s->device);
+    cudaDeviceSynchronize();
+    delete s;
+    return FG_OK;
+}
+
+int fg_solver_memory(const fg_solver *s, uint64_t *bytes) {
+    if (!s || !bytes) return set_err(FG_ERR_ARG, "fg_solver_memory: null argument");
+    *bytes = s->bytes;
+    return FG_OK;
+}
+
+#define FG_ENTER(s)                                                                   \
+    do {                                                                              \
+        if (!(s)) return set_err(FG_ERR_ARG, "null solver");                          \
+        if (cudaSetDevice((s)->device) != cudaSuccess) return set_err(FG_ERR_CUDA, "cudaSetDevice failed"); \
+    } while (0)
+
+int fg_set_state(fg_solver *s, const double *U, void *stream) {
+    FG_ENTER(s);
+    if (!U) return set_err(FG_ERR_ARG, "fg_set_state: null U");
+    return s->set_state(U, (cudaStream_t)stream);
+}
+int fg_get_state(fg_solver *s, double *U, void *stream) {
+    FG_ENTER(s);
+    if (!U) return set_err(FG_ERR_ARG, "fg_get_state: null U");
+    return s->get_state(U, (cudaStream_t)stream);
+}
+int fg_compute_rhs(fg_solver *s, int32_t want_signal, void *stream) {
+    FG_ENTER(s);
+    return s->compute_rhs(want_signal ? 1 : 0, (cudaStream_t)stream);
+}
+int fg_compute_time_step(fg_solver *s, double *dt_out, void *stream) {
+    FG_ENTER(s);
+    return s->time_step(dt_out, (cudaStream_t)stream);
+}
+int fg_init_rk(fg_solver *s, void *stream) {
+    FG_ENTER(s);
+    return s->init_rk((cudaStream_t)stream);
+}
+int fg_update(fg_solver *s, int32_t irk, void *stream) {
+    FG_ENTER(s);
+    if (irk < 0 || irk >= s->cs.rkSteps) return set_err(FG_ERR_ARG, "irk out of range");
+    return s->update(irk, 0, (cudaStream_t)stream);
+}
+int fg_stage(fg_solver *s, int32_t irk, void *stream) {
+    FG_ENTER(s);
+    if (irk < 0 || irk >= s->cs.rkSteps) return set_err(FG_ERR_ARG, "irk out of range");
+    return s->stage(irk, (s->cs.rkSteps == 3 && irk == 0) ? 1 : 0, (cudaStream_t)stream);
+}
+int fg_relaxation(fg_solver *s, fg_relax_stats *stats, void *stream) {
+    FG_ENTER(s);
+    return s->relax(stats, (cudaStream_t)stream);
+}
+int fg_cons_calc(fg_solver *s, int32_t ivar, double *out, void *stream) {
+    FG_ENTER(s);
+    if (ivar < 0 || ivar >= 10) return set_err(FG_ERR_ARG, "ivar out of range");
+    return s->cons(ivar, out, (cudaStream_t)stream);
+}
+int fg_get_time(fg_solver *s, double *dt, double *physicalTime, int32_t *iStep) {
+    FG_ENTER(s);
+    if (iStep) *iStep = s->iStep;
+    return s->get_time(dt, physicalTime);
+}
+int fg_set_dt(fg_solver *s, double dt) {
+    FG_ENTER(s);
+    return s->set_dt(dt);
+}
+
+int fg_step(fg_solver *s, void *stream) {
+    FG_ENTER(s);
+    cudaStream_t st = (cudaStream_t)stream;
+    const fg_case &c = s->cs;
+    int rc = s->advance_time(st);   // physicalTime += dt (previous dt, DP/explicitLoop.cu:29)
+    if (rc) return rc;
+    const int rk = c.rkSteps;
+    for (int irk = 0; irk < rk; irk++) {
+        const int writeU0 = (rk == 3 && irk == 0);
+        if (c.adaptDt == 1 && irk == 0 && s->iStep % c.adaptDtItr == 0) {
+            // residual with the signal speeds, new dt, then the stage update (DP/explicitLoop.cu:45-47)
+            if ((rc = s->compute_rhs(1, st))) return rc;
+            if ((rc = s->time_step(nullptr, st))) return rc;
+            if ((rc = s->update(irk, writeU0, st))) return rc;
+        } else {
+            if ((rc = s->stage(irk, writeU0, st))) return rc;
+        }
+    }
+    if (c.relaxFlag == 0)
+        if ((rc = s->relax(nullptr, st))) return rc;
+    if (c.consCalcFlag == 1 && s->iStep % c.adaptDtItr == 0)
+        if ((rc = s->cons(c.consCalcIvar, nullptr, st))) return rc;
+    s->iStep++;
+    return FG_OK;
+}
+
+int fg_profile(fg_solver *s, int32_t enable) {
+    FG_ENTER(s);
+    if (cudaDeviceSynchronize() != cudaSuccess) return set_err(FG_ERR_CUDA, "fg_profile: device error");
+    s->prof_reset(enable != 0);
+    return FG_OK;
+}
+int fg_profile_read(fg_solver *s, fg_kernel_times *out) {
+    FG_ENTER(s);
+    if (!out) return set_err(FG_ERR_ARG, "null output");
+    return s->prof_read(out);
+}
+int fg_launch_count(fg_solver *s, uint64_t *count) {
+    FG_ENTER(s);
+    if (!count) return set_err(FG_ERR_ARG, "null output");
+    *count = s->launches;
+    return FG_OK;
+}
+
+int fg_get_rhs(fg_solver *s, double *rhs) {
+    FG_ENTER(s);
+    if (!rhs) return set_err(FG_ERR_ARG, "null rhs");
+    return s->get_rhs(rhs);
+}
+int fg_get_limited(fg_solver *s, double *grad, double *theta) {
+    FG_ENTER(s);
+    return s->get_limited(grad, theta);
+}
+int fg_get_signal(fg_solver *s, double *signal) {
+    FG_ENTER(s);
+    if (!signal) return set_err(FG_ERR_ARG, "null signal");
+    return s->get_signal(signal);
+}
+
+}  // extern "C"

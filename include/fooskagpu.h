@@ -1,0 +1,250 @@
+/*
+ * fooskagpu.h — C ABI of the B200-native explicit residual path of the FooskaGPU
+ * two-phase finite-volume solver (one GPU, sm_100a).
+ *
+ * The reference has no plugin API: its boundary is the set of host stage functions that
+ * `explicitLoop` calls (mulitphase Solver/doublePrecision/strdata.h:206-247), operating on
+ * MESH / FIELD structs filled by `mainStart`.  Every entry point below replaces one of those
+ * functions (cited per declaration) with an opaque handle, plain pointers and sizes, and an
+ * integer status instead of `void` + printed CUDA errors.  No entry point aborts the process.
+ *
+ * Layout conventions at the boundary (what callers pass in and get back) are the reference's:
+ *   - conserved state U: AoS double, U[cell*10 + v], cells in .neu element order,
+ *     v = [alpha, alpha*rhoL, (1-alpha)*rhoG, rho*u, rho*v, rho*w,
+ *          alpha*rhoL*eL, (1-alpha)*rhoG*eG, rho*E, vapour mass]   (DP/initialize.cu:45-54)
+ *   - the device keeps its own renumbered SoA copy; conversion happens in fg_set_state /
+ *     fg_get_state.
+ */
+#ifndef FOOSKAGPU_H
+#define FOOSKAGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+enum fg_status_code {
+    FG_OK              = 0,
+    FG_ERR_ARG         = 1,  /* null pointer, out-of-range argument, size mismatch        */
+    FG_ERR_IO          = 2,  /* mesh / case file missing or unreadable                     */
+    FG_ERR_MESH        = 3,  /* malformed .neu, untagged open boundary, unmatched periodic */
+    FG_ERR_CUDA        = 4,  /* CUDA runtime error (message via fg_last_error)             */
+    FG_ERR_NAN         = 5,  /* non-finite value or non-positive density in the state      */
+    FG_ERR_UNSUPPORTED = 6,  /* option the build does not implement                        */
+    FG_ERR_NOMEM       = 7   /* device or host allocation failed                           */
+};
+
+/* Text of the last error raised on the calling thread (never NULL). */
+const char *fg_last_error(void);
+
+/* ---------------------------------------------------------------- case parameters
+ * Field-for-field the reference's `struct INPUT` (DP/strdata.h:49-98), same names, same
+ * meaning, same order.  Values are set by the caller (the reference hard-codes them in
+ * DP/buildInput.cu:10-69); fg_case_default() returns those hard-coded values.
+ * The trailing block holds options the reference lacks; zero selects reference behaviour. */
+typedef struct fg_case {
+    double  dt;
+    double  cfl;
+    int32_t adaptDt;
+    int32_t adaptDtItr;
+    double  maxDt;
+    double  avfMin;
+
+    int32_t rkSteps;
+    double  finalTime;
+    double  exportTime;
+    int32_t restartStep;
+    int32_t restartFlag;
+    int32_t neglectX;
+    int32_t neglectY;
+    int32_t neglectZ;
+    int32_t nMaterials;
+    int32_t NEQ;
+    double  scale;
+    int32_t viscFlag;
+    int32_t turbulence;
+    int32_t woodsFlag;
+
+    int32_t thermFntRlxFlag;
+    double  thermRlxRate;
+    double  thermUrf;
+    int32_t thermItrMax;
+
+    int32_t chemFlag;
+    int32_t chemFntRlxFlag;
+    double  chemRlxRate;
+    double  chemUrf;
+    int32_t chemItrMax;
+    int32_t chemCondesation;
+    double  chemLimit;
+
+    int32_t consCalcFlag;
+    int32_t consCalcIvar;
+
+    double  satTempUrf;
+
+    double  pInf[2];
+    double  gamma[2];
+    double  Cp[2];
+    double  eta[2];
+    double  satConst[2];
+    double  dynVisc[2];
+    double  heatCoef[2];
+    double  Pr[2];
+
+    /* ---- extensions (not in the reference; 0 = reference behaviour) ---- */
+    int32_t relaxFlag;      /* 0: relaxation every step as the reference; 1: skip relaxation */
+    int32_t reserved[7];
+} fg_case;
+
+/* Fill *c with the values the reference hard-codes in DP/buildInput.cu:10-69. */
+void fg_case_default(fg_case *c);
+
+/* ---------------------------------------------------------------- mesh
+ * Replaces translator_ptw + meshConnectivity + decompose(size 1) + buildLocalMesh +
+ * meshProperties (DP/translator.cu:3, DP/meshConnectivity.cu:175, DP/buildLocalMesh.cu:460,
+ * DP/meshProperties.cu:139).  Reads a Gambit neutral file with the reference's grammar,
+ * matches faces, computes the reference's geometry in FP64, builds the reference face order
+ * (owner = lower element index) and a locality-preserving renumbering for the device. */
+typedef struct fg_mesh fg_mesh;
+
+enum fg_renumber { FG_RENUMBER_NONE = 0, FG_RENUMBER_MORTON = 1, FG_RENUMBER_RCM = 2 };
+
+typedef struct fg_mesh_opts {
+    double  scale;        /* coordinates are multiplied by this (reference: input.scale)   */
+    double  periodic[3];  /* >0: box length of a periodic axis (extension; 0 = none)       */
+    int32_t renumber;     /* enum fg_renumber for the device ordering                      */
+    int32_t reserved[3];
+} fg_mesh_opts;
+
+typedef struct fg_mesh_info {
+    int32_t nElem;        /* cells                                                          */
+    int32_t nNodes;
+    int32_t nFcs;         /* faces (interior + boundary), reference face order              */
+    int32_t nBoundary;    /* faces with boundCond != 0                                      */
+    int32_t nPeriodic;    /* interior faces formed by periodic matching                     */
+    int32_t maxFaces;     /* max faces per cell (4 tet, 5 prism/pyramid, 6 hex)             */
+    int32_t nTet, nPyr, nPrism, nHex;
+} fg_mesh_info;
+
+/* Read-only views of the reference-layout host arrays (valid until fg_mesh_free).
+ * fc2el[f*2+s], boundCond[f], cellCenter[c*3+d], fcCenter[f*3+d], n/nt1/nt2[f*3+d],
+ * area[f], volume[c]  — the arrays of the reference's MESH struct (DP/strdata.h:100-115).
+ * nbShift[f*3+d] is the periodic image offset of face f seen from its neighbour (0 if none). */
+typedef struct fg_mesh_view {
+    int32_t nElem, nFcs;
+    const int32_t *fc2el;
+    const int32_t *boundCond;
+    const double  *cellCenter;
+    const double  *fcCenter;
+    const double  *n, *nt1, *nt2;
+    const double  *area;
+    const double  *volume;
+    const double  *nbShift;
+} fg_mesh_view;
+
+int  fg_mesh_load_neu(const char *path, const fg_mesh_opts *opts, fg_mesh **out);
+int  fg_mesh_info_get(const fg_mesh *m, fg_mesh_info *info);
+int  fg_mesh_view_get(const fg_mesh *m, fg_mesh_view *view);
+/* new2old[i] = reference (.neu) index of device cell i. */
+int  fg_mesh_permutation(const fg_mesh *m, int32_t *new2old, int32_t n);
+void fg_mesh_free(fg_mesh *m);
+
+/* ---------------------------------------------------------------- solver context
+ * Replaces startDevice (DP/startDevice.cu:14): allocates every device array once. */
+typedef struct fg_solver fg_solver;
+
+enum fg_precision {
+    FG_PREC_FP64  = 0,   /* FP64 everywhere ("plain" path)                                       */
+    FG_PREC_MIXED = 1    /* FP32 reconstruction / HLLC / WALE / viscous; FP64 state, RK, dt, Newton */
+};
+
+int fg_solver_create(const fg_mesh *m, const fg_case *c, int32_t precision, int32_t device,
+                     fg_solver **out);
+int fg_solver_destroy(fg_solver *s);
+/* Device bytes held by the solver (mesh + field arrays). */
+int fg_solver_memory(const fg_solver *s, uint64_t *bytes);
+
+/* Replaces initialize / readField (DP/initialize.cu:61, DP/restart.cu:424): upload U
+ * (nElem*10 doubles, reference order) from host memory.  stream may be NULL. */
+int fg_set_state(fg_solver *s, const double *U, void *stream);
+/* Download U (nElem*10 doubles, reference order).  Synchronises `stream`. */
+int fg_get_state(fg_solver *s, double *U, void *stream);
+
+/* ---------------------------------------------------------------- stage functions */
+
+/* computePrimVec + computeGrad + computeFaceValues(limiter) + computeRHS (+ viscous)
+ * (DP/computePrimVec.cu:82, DP/computeGrad.cu:263, DP/computeFaceValues.cu:138,
+ *  DP/computeRHS.cu:384): residual of the current state into the device RHS buffer.
+ * With want_signal != 0 also the per-cell max signal speed used by computeTimeStep. */
+int fg_compute_rhs(fg_solver *s, int32_t want_signal, void *stream);
+
+/* computeTimeStep (DP/computeTimeStep.cu:172): after fg_compute_rhs(want_signal=1),
+ * dt = min(cfl * min_c V^0.3333 / s_c, maxDt), kept on the device; *dt_out (may be NULL)
+ * receives it (synchronises the stream when non-NULL). */
+int fg_compute_time_step(fg_solver *s, double *dt_out, void *stream);
+
+/* initRk (DP/update.cu:141): U0 = U. */
+int fg_init_rk(fg_solver *s, void *stream);
+
+/* update (DP/update.cu:105): Runge-Kutta stage irk from the RHS buffer with the device dt. */
+int fg_update(fg_solver *s, int32_t irk, void *stream);
+
+/* One full RK stage irk with the fused residual + update kernel (no RHS buffer round trip). */
+int fg_stage(fg_solver *s, int32_t irk, void *stream);
+
+/* relaxation (DP/relaxation.cu:77): partition + thermal + chemical equilibrium (FP64 Newton). */
+typedef struct fg_relax_stats {
+    int32_t nTherm;       /* cells relaxed thermally          */
+    int32_t nChem;        /* cells relaxed chemically         */
+    int32_t nAbort;       /* Newton solves that fell back to the best iterate */
+    int32_t reserved;
+} fg_relax_stats;
+int fg_relaxation(fg_solver *s, fg_relax_stats *stats, void *stream);
+
+/* consCalc (DP/consCalc.cu:40): FP64 integral of variable ivar over the domain
+ * (ivar 0 integrates 1-alpha).  Deterministic two-level reduction. */
+int fg_cons_calc(fg_solver *s, int32_t ivar, double *out, void *stream);
+
+/* dt and physical time held by the solver. */
+int fg_get_time(fg_solver *s, double *dt, double *physicalTime, int32_t *iStep);
+int fg_set_dt(fg_solver *s, double dt);
+
+/* One explicitLoop iteration (DP/explicitLoop.cu:28-64): time advance, RK stages with the
+ * adaptive dt at stage 0 every adaptDtItr steps, relaxation, conservation every adaptDtItr. */
+int fg_step(fg_solver *s, void *stream);
+
+/* ---------------------------------------------------------------- instrumentation
+ * (the reference has per-phase cudaEvent timers commented out, e.g. DP/computeRHS.cu:221-235)
+ * With profiling enabled every kernel launch of the solver is bracketed by CUDA events on the
+ * stream it is launched on; fg_profile_read synchronises and returns per-kind totals.
+ * Kinds: 0 gradient+limiter, 1 flux+gather+RK, 2 RK update, 3 relaxation, 4 dt reduction,
+ *        5 conservation, 6 other (state copies, time advance). */
+enum { FG_K_GRAD = 0, FG_K_FLUX = 1, FG_K_UPDATE = 2, FG_K_RELAX = 3, FG_K_DT = 4, FG_K_CONS = 5, FG_K_OTHER = 6,
+       FG_K_NKINDS = 8 };
+typedef struct fg_kernel_times {
+    double  ms[FG_K_NKINDS];
+    int64_t launches[FG_K_NKINDS];
+} fg_kernel_times;
+int fg_profile(fg_solver *s, int32_t enable);                 /* enable (1) / disable (0); resets */
+int fg_profile_read(fg_solver *s, fg_kernel_times *out);
+/* Number of kernels the solver has launched since creation. */
+int fg_launch_count(fg_solver *s, uint64_t *count);
+
+/* ---------------------------------------------------------------- parity hooks
+ * Copies of intermediate device buffers in reference order, for tests.
+ *   fg_get_rhs:    RHS[nElem*10]            (after fg_compute_rhs)
+ *   fg_get_limited: grad[nElem*10*3] and theta[nElem*10] of the last residual (vars 0..8;
+ *                   var 9, the mixture density the reference also limits but never uses,
+ *                   is returned as 0)
+ *   fg_get_signal: per-cell max signal speed of the last fg_compute_rhs(want_signal=1) */
+int fg_get_rhs(fg_solver *s, double *rhs);
+int fg_get_limited(fg_solver *s, double *grad, double *theta);
+int fg_get_signal(fg_solver *s, double *signal);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FOOSKAGPU_H */

@@ -1,0 +1,59 @@
+"""Small meshes and cases shared by the GPU parity tests."""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+from fooskagpu_b200 import cases, meshgen
+from fooskagpu_b200.api import Mesh
+
+ALL_BC = {"x0": "inlet", "x1": "outlet", "y0": "wall", "y1": "slip", "z0": "symmetry", "z1": "slip"}
+SLIP = {s: "slip" for s in ("x0", "x1", "y0", "y1", "z0", "z1")}
+
+
+def make(name: str, meshdir) -> tuple:
+    """Return (Mesh, case, U0) for a named parity case."""
+    path = os.path.join(str(meshdir), name + ".neu")
+    periodic = (0.0, 0.0, 0.0)
+    if name == "tet_ref":
+        if not os.path.exists(path):
+            meshgen.write_neu(path, meshgen.box_tets(6, 3, 3, L=(0.006, 0.003, 0.003), origin=(-0.003, 0, 0),
+                                                     jitter=0.1, side_bc=ALL_BC))
+        c = cases.reference_case()
+        ic = "perturbed"
+    elif name == "mixed_ref_rk3":
+        if not os.path.exists(path):
+            meshgen.write_neu(path, meshgen.box_mixed(4, 4, 3, L=(0.004, 0.004, 0.003), side_bc=SLIP))
+        c = cases.reference_case()
+        c.rkSteps = 3
+        ic = "perturbed"
+    elif name == "hex_periodic_tgv":
+        L = 2 * math.pi
+        if not os.path.exists(path):
+            meshgen.write_neu(path, meshgen.box_hexes(8, 8, 8, L=(L, L, L), side_bc={}, shuffle=True))
+        periodic = (L, L, L)
+        c = cases.tgv_case()
+        c.adaptDtItr = 2
+        ic = "tgv"
+    elif name == "tet_sod":
+        if not os.path.exists(path):
+            meshgen.write_neu(path, meshgen.box_tets(24, 3, 3, L=(1.0, 0.1, 0.1), jitter=0.1, side_bc=SLIP))
+        c = cases.sod_case()
+        c.adaptDtItr = 2
+        ic = "sod"
+    else:
+        raise KeyError(name)
+    m = Mesh.load_neu(path, scale=1.0, periodic=periodic)
+    a = m.arrays()
+    if ic == "perturbed":
+        U = cases.perturbed_two_phase_ic(c, a["cellCenter"], seed=5, vel=25.0)
+    elif ic == "tgv":
+        U = cases.tgv_ic(c, a["cellCenter"])
+    else:
+        U = cases.sod_ic(c, a["cellCenter"])
+    return m, c, U
+
+
+NAMES = ["tet_ref", "mixed_ref_rk3", "hex_periodic_tgv", "tet_sod"]

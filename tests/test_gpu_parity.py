@@ -1,0 +1,175 @@
+"""Parity of the device path (through the C ABI) with the CPU oracle.
+
+Tolerances (per variable, max |gpu - oracle| / max |oracle|):
+  FP64 path   : 1e-9 for residuals / gradients, 1e-10 for states after a few steps — the only
+                differences are summation order (cell gathers vs face-order scatter), FMA
+                contraction and the algebraic identities that replace the tangent frame.
+  mixed path  : FP32 reconstruction / HLLC / viscous flux: 2e-4 for residuals, 3e-4 for
+                limited gradients, 2e-6 for states after a few steps (FP64 update).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from gpu_cases import NAMES, make
+from oracle.oracle_py import Oracle
+from fooskagpu_b200.api import Solver
+
+pytestmark = pytest.mark.gpu
+
+TOL = {
+    "fp64": {"rhs": 1e-9, "grad": 1e-9, "theta": 1e-9, "signal": 1e-12, "dt": 1e-12, "state": 1e-10, "relax": 1e-11},
+    "mixed": {"rhs": 2e-4, "grad": 3e-4, "theta": 1e-3, "signal": 2e-6, "dt": 2e-6, "state": 2e-6, "relax": 1e-11},
+}
+REPORT = os.environ.get("FG_PARITY_REPORT")
+
+
+def _report(key, val):
+    if not REPORT:
+        return
+    d = {}
+    if os.path.exists(REPORT):
+        d = json.load(open(REPORT))
+    d[key] = val
+    json.dump(d, open(REPORT, "w"), indent=1)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", NAMES)
+def test_residual(name, prec, meshdir):
+    m, c, U = make(name, meshdir)
+    o = Oracle(m.view(), c)
+    R_o = o.residual(U)
+    smin_o = o.timestep_min()
+    s = Solver(m, c, precision=prec)
+    s.set_state(U)
+    s.compute_rhs(want_signal=True)
+    R_g = s.get_rhs()
+    g_g, th_g = s.get_limited()
+    sig_g = s.get_signal()
+    dt_g = s.compute_time_step()
+    dt_o = min(c.cfl * smin_o, c.maxDt)
+    e_rhs = rel_err(R_g, R_o)
+    e_grad = rel_err(g_g[:, :9].reshape(len(U), -1), o.grad[:, :9].reshape(len(U), -1))
+    e_th = np.abs(th_g[:, :9] - o.theta[:, :9]).max()
+    e_sig = rel_err(sig_g, o.signal)
+    e_dt = abs(dt_g - dt_o) / dt_o
+    _report(f"residual/{name}/{prec}", dict(rhs=e_rhs.tolist(), grad=float(e_grad.max()), theta=float(e_th),
+                                            signal=float(e_sig), dt=e_dt))
+    t = TOL[prec]
+    assert e_rhs.max() < t["rhs"], e_rhs
+    assert e_grad.max() < t["grad"], e_grad
+    assert e_th < t["theta"], e_th
+    assert e_sig < t["signal"]
+    assert e_dt < t["dt"]
+    s.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", NAMES)
+def test_steps(name, prec, meshdir):
+    """Three explicitLoop steps (RK stages, adaptive dt, relaxation, conservation)."""
+    m, c, U = make(name, meshdir)
+    o = Oracle(m.view(), c)
+    Uo = U.copy()
+    s = Solver(m, c, precision=prec)
+    s.set_state(U)
+    nsteps = 3
+    for _ in range(nsteps):
+        o.step(Uo)
+        s.step()
+    Ug = s.get_state()
+    dt_g, t_g, it_g = s.time()
+    e = rel_err(Ug, Uo)
+    _report(f"steps/{name}/{prec}", dict(state=e.tolist(), dt=abs(dt_g - o.dt.value) / o.dt.value))
+    assert it_g == nsteps
+    assert abs(dt_g - o.dt.value) <= TOL[prec]["dt"] * o.dt.value
+    assert abs(t_g - o.time.value) <= TOL[prec]["dt"] * max(o.time.value, 1e-300) * nsteps
+    assert e.max() < TOL[prec]["state"], e
+    s.close()
+
+
+@pytest.mark.parametrize("name", ["tet_ref", "mixed_ref_rk3"])
+def test_relaxation(name, meshdir):
+    m, c, U = make(name, meshdir)
+    o = Oracle(m.view(), c)
+    Uo = U.copy()
+    st_o = o.relaxation(Uo)
+    s = Solver(m, c, precision="fp64")
+    s.set_state(U)
+    st_g = s.relaxation()
+    Ug = s.get_state()
+    e = rel_err(Ug, Uo)
+    _report(f"relax/{name}", dict(state=e.tolist(), oracle=st_o, gpu=st_g))
+    assert st_g["nChem"] == st_o["nChem"] and st_g["nTherm"] == st_o["nTherm"]
+    assert st_o["nChem"] > 0, "fixture should exercise the chemical branch"
+    assert e.max() < TOL["fp64"]["relax"], e
+    s.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_cons_calc(name, meshdir):
+    m, c, U = make(name, meshdir)
+    o = Oracle(m.view(), c)
+    s = Solver(m, c, precision="fp64")
+    s.set_state(U)
+    for iv in (0, 1, 8, 9):
+        a, b = s.cons_calc(iv), o.cons_calc(iv, U)
+        assert abs(a - b) <= 1e-13 * max(abs(b), 1e-300), (iv, a, b)
+    s.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_deterministic(prec, meshdir):
+    """No atomics on the data path: two runs give bitwise identical states."""
+    m, c, U = make("tet_ref", meshdir)
+    out = []
+    for _ in range(2):
+        s = Solver(m, c, precision=prec)
+        s.set_state(U)
+        for _ in range(3):
+            s.step()
+        out.append(s.get_state())
+        s.close()
+    assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_periodic_conservation(prec, meshdir):
+    """Periodic TGV: partial masses, total energy and vapour mass are conserved to round-off
+    (both cells of a face evaluate its flux identically, so contributions cancel exactly)."""
+    m, c, U = make("hex_periodic_tgv", meshdir)
+    s = Solver(m, c, precision=prec)
+    s.set_state(U)
+    before = [s.cons_calc(iv) for iv in (1, 2, 8)]
+    for _ in range(5):
+        s.step()
+    after = [s.cons_calc(iv) for iv in (1, 2, 8)]
+    for b, a in zip(before, after):
+        assert abs(a - b) <= 1e-12 * abs(b), (a, b)
+    s.close()
+
+
+def test_stage_api_matches_step(meshdir):
+    """fg_init_rk + fg_compute_rhs + fg_update per stage equals the fused fg_stage path."""
+    m, c, U = make("mixed_ref_rk3", meshdir)
+    c.adaptDt = 0
+    c.dt = 1e-9
+    c.relaxFlag = 1
+    c.consCalcFlag = 0
+    a = Solver(m, c, precision="fp64")
+    b = Solver(m, c, precision="fp64")
+    a.set_state(U)
+    b.set_state(U)
+    b.init_rk()
+    for irk in range(3):
+        a.stage(irk)
+        b.compute_rhs()
+        b.update(irk)
+    Ua, Ub = a.get_state(), b.get_state()
+    assert np.array_equal(Ua, Ub)
+    a.close()
+    b.close()
