@@ -35,7 +35,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "cell-updates/s (cells×RK stages/s) at 1 B200, mixed+surrogate vs FP64 plain; %HBM peak"
 UNIT = "cell-updates/s"
-NCELL_SIDE = 128
+NCELL_SIDE = int(os.environ.get("FG_BENCH_N", "128"))
 MESH_DIR = Path(os.environ.get("FG_BENCH_MESH_DIR", tempfile.gettempdir())) / "fooskagpu_bench"
 
 
@@ -340,7 +340,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-stages", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--n", type=int, default=None, help="cells per side of the TGV cube (default 128)")
     args = ap.parse_args()
+    if args.n:
+        global NCELL_SIDE
+        NCELL_SIDE = args.n
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

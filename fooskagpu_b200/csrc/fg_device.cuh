@@ -29,7 +29,8 @@ struct PhysT {
     T chemLimit;
     // inlet ghost state (DP/bc.h:2-25), precomputed in FP64 on the host
     T inAlpha, inRhoL, inRhoG, inP;
-    int woods, visc, turb;
+    T tieTol;      // |S*| <= tieTol (|S_L| + |S_R|) counts as S* = 0 (extension; 0 = reference)
+    int woods, visc, turb, energyFix;
 };
 
 struct PhysD {
@@ -131,7 +132,7 @@ __device__ __forceinline__ void hllc_flux(const PhysT<T> &P, const T *L, const T
     const T rL = L[0] * L[1] + (1 - L[0]) * L[2];
     const T rR = R[0] * R[1] + (1 - R[0]) * R[2];
     const T Ss = (pmR - pmL + rL * uL * (SL - uL) - rR * uR * (SR - uR)) / (rL * (SL - uL) - rR * (SR - uR));
-    const bool left = (Ss >= 0);
+    const bool left = (Ss >= 0) || (P.tieTol > 0 && fabs(Ss) <= P.tieTol * (fabs(SL) + fabs(SR)));
     const bool star = (SL < 0) && (SR >= 0);
     T s[NP];
 #pragma unroll
@@ -166,7 +167,8 @@ __device__ __forceinline__ void hllc_flux(const PhysT<T> &P, const T *L, const T
         const T pSG = (s[7] + P.pinf[1]) * (P.gm1[1] * s[2] - P.gp1[1] * rSG) / (P.gm1[1] * rSG - P.gp1[1] * s[2]) - P.pinf[1];
         ar6 = v1 * eos_e(P, 0, pSL, rSL);
         ar7 = v2 * eos_e(P, 1, pSG, rSG);
-        const T v8 = fac * (c8 + du * (Ss + pm / (rho * (cK - un))));
+        // reference energy star state (DP/starRegion.h:29); energyFix restores the rho_K factor
+        const T v8 = fac * (c8 + (P.energyFix ? rho : (T)1) * du * (Ss + pm / (rho * (cK - un))));
         const T v9 = s[8] * fac;
         h1 = cK * (v1 - c1);
         h2 = cK * (v2 - c2);
@@ -212,7 +214,7 @@ __device__ __forceinline__ T wale_nu(const T *g, T volAvg) {
         }
     const T r1 = sqrt(s1), r2 = sqrt(s2);
     T num = s1 * r1;                       // s1^1.5
-    const T den = r1 * sqrt(r1) + s2 * s2 * r2 + (T)1e-12;  // s1^1.25 + s2^2.5 + 1e-12
+    const T den = s1 * sqrt(r1) + s2 * s2 * r2 + (T)1e-12;  // s1^1.25 + s2^2.5 + 1e-12
     if (den < (T)1e-10) num = 0;
     const T Ls = (T)0.325 * cbrt(volAvg);
     return Ls * Ls * num / den;

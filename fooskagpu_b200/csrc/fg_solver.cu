@@ -180,6 +180,8 @@ struct SolverT : public fg_solver {
         P.woods = (cs.woodsFlag == 1);
         P.visc = (cs.viscFlag == 1);
         P.turb = (cs.turbulence == 1);
+        P.energyFix = (cs.hllcEnergyFix == 1);
+        P.tieTol = (T)cs.hllcTieTol;
         {
             // inlet ghost (DP/bc.h:2-25): rho from p = 11.4e5 Pa, T = 115.3 K
             const double pIn = 11.4e5, tIn = 115.3;

@@ -96,7 +96,16 @@ typedef struct fg_case {
 
     /* ---- extensions (not in the reference; 0 = reference behaviour) ---- */
     int32_t relaxFlag;      /* 0: relaxation every step as the reference; 1: skip relaxation */
-    int32_t reserved[7];
+    /* The reference's HLLC energy star state (DP/starRegion.h:29) lacks the rho_K factor on its
+     * second term, so the energy flux jumps at S* = 0 (left branch: u_L p_L (1 - 1/rho_L),
+     * right branch: its mirror).  Where S* = 0 in exact arithmetic (slip walls, symmetry planes)
+     * round-off picks the branch, in the reference as well.
+     *   hllcEnergyFix = 1 uses the standard HLLC energy star state (continuous at S* = 0);
+     *   hllcTieTol > 0 treats |S*| <= hllcTieTol * (|S_L| + |S_R|) as S* = 0 (left state), which
+     *   makes two implementations with different rounding take the same branch. */
+    int32_t hllcEnergyFix;
+    double  hllcTieTol;
+    int32_t reserved[4];
 } fg_case;
 
 /* Fill *c with the values the reference hard-codes in DP/buildInput.cu:10-69. */

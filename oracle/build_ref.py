@@ -79,7 +79,10 @@ def build_gpu(ref: Path = DEFAULT_REF, force: bool = False) -> Path:
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     objdir = OUT / "gpu_obj"
     objdir.mkdir(exist_ok=True)
-    flags = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true", "--expt-relaxed-constexpr",
+    # the reference launches 512-thread blocks; its flux kernel needs ~166 registers, which
+    # exceeds the 64K-register file per block on sm_100a ("too many resources requested for
+    # launch"), so registers are capped at 128 (= 65536 / 512) as a build flag
+    flags = ["-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-rdc=true", "--expt-relaxed-constexpr", "-maxrregcount=128",
              "-Xcompiler", "-fopenmp", "-I", str(SHIM), "-I", str(dp)]
     objs = []
     for t in GPU_TUS:

@@ -185,7 +185,10 @@ void star_region(const fg_case *c, const double *s, const double *ul, double SK,
     consF[7] = vS[2] * eqos(c, 1, 3, pSG, rSG);
     const double p = s[0] * s[6] + (1 - s[0]) * s[7];
     const double r = s[0] * s[1] + (1 - s[0]) * s[2];
-    vS[8] = ((SK - ul[0]) / (SK - SS)) * (consF[8] + (SS - ul[0]) * (SS + p / (r * (SK - ul[0]))));
+    if (c->hllcEnergyFix == 1)   /* standard HLLC energy star state (extension) */
+        vS[8] = ((SK - ul[0]) / (SK - SS)) * (consF[8] + r * (SS - ul[0]) * (SS + p / (r * (SK - ul[0]))));
+    else
+        vS[8] = ((SK - ul[0]) / (SK - SS)) * (consF[8] + (SS - ul[0]) * (SS + p / (r * (SK - ul[0]))));
     vS[9] = s[8] * (SK - ul[0]) / (SK - SS);
 }
 
@@ -258,7 +261,8 @@ void face_flux(const fg_case *c, const double *n, const double *t1, const double
                double *out) {
     double cs[3], uL[3], uR[3];
     wave_speeds(c, n, t1, t2, solL, solR, cs, uL, uR);
-    const int isLeft = (cs[1] >= 0);
+    int isLeft = (cs[1] >= 0);
+    if (c->hllcTieTol > 0 && fabs(cs[1]) <= c->hllcTieTol * (fabs(cs[0]) + fabs(cs[2]))) isLeft = 1;
     const int isStar = (cs[0] < 0 && cs[2] >= 0);
     const double *s = isLeft ? solL : solR;
     const double *vl = isLeft ? uL : uR;

@@ -209,7 +209,7 @@ def ic_for(spec, c, centres):
 def write_case_file(path, c):
     with open(path, "w") as f:
         for k, t in type(c)._fields_:
-            if k in ("relaxFlag", "reserved"):
+            if k in ("relaxFlag", "hllcEnergyFix", "hllcTieTol", "reserved"):
                 continue
             v = getattr(c, k)
             if hasattr(v, "__len__"):
@@ -228,7 +228,7 @@ def centres_of(mesh: meshgen.NeuMesh):
 
 def run_stage_fixtures(outdir):
     exe = ROOT / "oracle" / "_ref" / "fooska_ref_dp"
-    outdir = Path(outdir)
+    outdir = Path(outdir).resolve()
     for spec in stage_specs():
         wd = outdir / spec["name"]
         wd.mkdir(parents=True, exist_ok=True)
