@@ -58,6 +58,10 @@ def build_product(force: bool = False, verbose: bool = False) -> Path:
     for s in cu:
         o = objdir / (s.stem + ".o")
         cmd = [nvcc, *ARCH, "-lineinfo", *common, "-c", str(s), "-o", str(o)]
+        if s.name == "fg_kernels.cu":
+            # the stage kernels' FP32 face math uses fast division / square root / FTZ (the FP32
+            # path's tolerance allows ~2 ulp); FP64 code is unaffected by these flags
+            cmd.insert(1, "--use_fast_math")
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         out = _run(cmd)

@@ -80,25 +80,53 @@ __device__ __forceinline__ void store_g<float>(float *G, int c, const float *g) 
     for (int q = 0; q < GREC / 4; q++) p[q] = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
 }
 
+// ------------------------------------------------------------------ lane groups
+// A cell is handled by a group of G lanes (G = 4 for tetrahedra, 8 when a cell can have 5 or 6
+// faces); lane k of the group works on the face in slot k.  Partial results are combined with
+// a butterfly of warp shuffles inside the group, whose order is fixed — so results are
+// deterministic — and every lane ends with the cell total.
+template <int G, typename X>
+__device__ __forceinline__ X group_sum(X v) {
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off, G);
+    return v;
+}
+template <int G, typename X>
+__device__ __forceinline__ X group_min(X v) {
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off, G));
+    return v;
+}
+template <int G, typename X>
+__device__ __forceinline__ X group_max(X v) {
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off, G));
+    return v;
+}
+
 // ------------------------------------------------------------------ gradient + limiter
-template <typename T>
+template <typename T, int G>
 __global__ void __launch_bounds__(kGradThreads) k_grad(const DevMesh<T> m, const T *__restrict__ W,
-                                                       T *__restrict__ G, const PhysT<T> P) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.n) return;
-    const int n = m.n;
-    T w[NP], gs[NP * 3], mn[NP], mx[NP];
-    load_rec(W, c, w);
+                                                       T *__restrict__ G_, const PhysT<T> P) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = gid / G;
+    const int k = gid % G;
+    const bool cell = c < m.n;     // uniform across the group
+    const int cc = cell ? c : m.n - 1;
+    T w[NP];
+    load_rec(W, cc, w);
+    const int fl = m.flags[cc];
+    const int nf = fl & 7;
+    const bool act = cell && k < nf;
+    const size_t o = (size_t)cc * m.nSlots + (act ? k : 0);
+    T gs[NP * 3], mn[NP], mx[NP];
 #pragma unroll
     for (int v = 0; v < NP; v++) {
         gs[3 * v] = gs[3 * v + 1] = gs[3 * v + 2] = 0;
         mn[v] = (T)1e12;
         mx[v] = (T)-1e12;
     }
-    const int fl = m.flags[c];
-    const int nf = fl & 7;
-    for (int k = 0; k < nf; k++) {
-        const size_t o = (size_t)k * n + c;
+    if (act) {
         const int nb = m.nbr[o];
         const T nx = m.nx[o], ny = m.ny[o], nz = m.nz[o], A = m.A[o];
         const T sg = ((fl >> (3 + k)) & 1) ? (T)1 : (T)-1;   // outward orientation of this cell
@@ -113,23 +141,27 @@ __global__ void __launch_bounds__(kGradThreads) k_grad(const DevMesh<T> m, const
         const T ax = sg * nx * A, ay = sg * ny * A, az = sg * nz * A;
 #pragma unroll
         for (int v = 0; v < NP; v++) {
-            mx[v] = fmax(mx[v], ot[v]);
-            mn[v] = fmin(mn[v], ot[v]);
+            mx[v] = ot[v];
+            mn[v] = ot[v];
             const T h = (w[v] + ot[v]) * (T)0.5;
-            gs[3 * v + 0] += h * ax;
-            gs[3 * v + 1] += h * ay;
-            gs[3 * v + 2] += h * az;
+            gs[3 * v + 0] = h * ax;
+            gs[3 * v + 1] = h * ay;
+            gs[3 * v + 2] = h * az;
         }
     }
-    const T iv = (T)(1.0 / m.vol[c]);
+    const T iv = (T)(1.0 / m.vol[cc]);
 #pragma unroll
-    for (int q = 0; q < NP * 3; q++) gs[q] *= iv;
+    for (int q = 0; q < NP * 3; q++) gs[q] = group_sum<G>(gs[q]) * iv;
+#pragma unroll
+    for (int v = 0; v < NP; v++) {
+        mn[v] = group_min<G>(mn[v]);
+        mx[v] = group_max<G>(mx[v]);
+    }
     // limiter (DP/computeFaceValues.cu:66-81): theta = min over faces of clamp(phi, 0, 1)
     T th[NP];
 #pragma unroll
     for (int v = 0; v < NP; v++) th[v] = (T)1e9;
-    for (int k = 0; k < nf; k++) {
-        const size_t o = (size_t)k * n + c;
+    if (act) {
         const T dx = m.dcx[o], dy = m.dcy[o], dz = m.dcz[o];
 #pragma unroll
         for (int v = 0; v < NP; v++) {
@@ -138,15 +170,26 @@ __global__ void __launch_bounds__(kGradThreads) k_grad(const DevMesh<T> m, const
             const T diff = wun - w[v];
             T phi = 1;
             if (diff != 0) phi = ((wun > w[v]) ? (mx[v] - w[v]) : (mn[v] - w[v])) / (2 * diff);
-            th[v] = fmin(th[v], fmax((T)0, fmin(phi, (T)1)));
+            th[v] = fmax((T)0, fmin(phi, (T)1));
         }
     }
-    T out[GREC];
 #pragma unroll
-    for (int v = 0; v < NP; v++) out[v] = th[v];
+    for (int v = 0; v < NP; v++) th[v] = group_min<G>(th[v]);
+    if (cell) {
+        // the record [theta(9), grad(27)] is written by the lanes of the group in 4-word pieces
+        T rec[GREC];
 #pragma unroll
-    for (int q = 0; q < NP * 3; q++) out[NP + q] = gs[q];
-    store_g(G, c, out);
+        for (int v = 0; v < NP; v++) rec[v] = th[v];
+#pragma unroll
+        for (int q = 0; q < NP * 3; q++) rec[NP + q] = gs[q];
+        T *dst = G_ + (size_t)c * GREC;
+#pragma unroll
+        for (int piece = 0; piece < GREC / 4; piece++)
+            if (piece % G == k) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) dst[4 * piece + j] = rec[4 * piece + j];
+            }
+    }
 }
 
 // MUSCL face state of a cell: w + theta * ((x_f - x_c) . grad w)  (DP/computeFaceValues.cu:66-105)
@@ -160,125 +203,149 @@ __device__ __forceinline__ void face_state(const T *w, const T *g, T dx, T dy, T
 }
 
 // ------------------------------------------------------------------ flux + gather + RK
-template <typename T>
+template <typename T, int G>
 __global__ void __launch_bounds__(kFluxThreads) k_flux(const DevMesh<T> m, Fields<T> f, const PhysT<T> P,
                                                        const PhysD D, int mode, int wantSignal, StageCoef sc) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = gid / G;
+    const int k = gid % G;
     const int n = m.n;
-    double cfl = 1e12;   // per-cell CFL bound for the block minimum
-    if (c < n) {
-        T w[NP], g[GREC];
-        load_rec(f.Win, c, w);
-        load_g(f.G, c, g);
-        const T pc = w[0] * w[6] + (1 - w[0]) * w[7];
-        double acc[NV];
+    const bool cell = c < n;
+    const int cc = cell ? c : n - 1;
+    const int fl = m.flags[cc];
+    const int nf = fl & 7;
+    const bool act = cell && k < nf;
+    T w[NP];
+    load_rec(f.Win, cc, w);
+    T cb[NV];
 #pragma unroll
-        for (int v = 0; v < NV; v++) acc[v] = 0.0;
-        T sig = (T)-1e9;
-        const int fl = m.flags[c];
-        const int nf = fl & 7;
-        const double vc = m.vol[c];
-        for (int k = 0; k < nf; k++) {
-            const size_t o = (size_t)k * n + c;
-            const int nb = m.nbr[o];
-            const bool own = (fl >> (3 + k)) & 1;
-            const T nx = m.nx[o], ny = m.ny[o], nz = m.nz[o], A = m.A[o];
-            T sc_[NP], so[NP];   // own and other reconstructed face states
+    for (int v = 0; v < NV; v++) cb[v] = 0;
+    T sig = (T)-1e9;
+    const double vc = m.vol[cc];
+    if (act) {
+        const size_t o = (size_t)cc * m.nSlots + k;
+        const int nb = m.nbr[o];
+        const bool own = (fl >> (3 + k)) & 1;
+        const T nx = m.nx[o], ny = m.ny[o], nz = m.nz[o], A = m.A[o];
+        T sc_[NP], so[NP];   // own and other reconstructed face states
+        T gO[9], gN[9];      // velocity gradients of owner / neighbour (viscous)
+        T p1[NP];            // slot-1 state as the viscous kernel reads it
+        T vAvg;
+        {
+            T g[GREC];
+            load_g(f.G, cc, g);
             face_state(w, g, m.dcx[o], m.dcy[o], m.dcz[o], sc_);
-            T gO[9], gN[9];      // velocity gradients of owner / neighbour (viscous)
-            T p1[NP];            // slot-1 state as the viscous kernel reads it
-            T vAvg;
-            if (nb >= 0) {
-                T wn[NP], gn[GREC];
-                load_rec(f.Win, nb, wn);
-                load_g(f.G, nb, gn);
-                face_state(wn, gn, m.dnx[o], m.dny[o], m.dnz[o], so);
 #pragma unroll
-                for (int q = 0; q < 9; q++) {
-                    gO[q] = own ? g[NP + 9 + q] : gn[NP + 9 + q];
-                    gN[q] = own ? gn[NP + 9 + q] : g[NP + 9 + q];
-                }
-                vAvg = (T)((own ? (vc + m.vol[nb]) : (m.vol[nb] + vc)) * 0.5);
-            } else {
-                // ghost of the reconstructed state for the flux (DP/computeRHS.cu:113)
+            for (int q = 0; q < 9; q++) gO[q] = g[NP + 9 + q];
+        }
+        if (nb >= 0) {
+            T wn[NP], gn[GREC];
+            load_rec(f.Win, nb, wn);
+            load_g(f.G, nb, gn);
+            face_state(wn, gn, m.dnx[o], m.dny[o], m.dnz[o], so);
 #pragma unroll
-                for (int v = 0; v < NP; v++) so[v] = sc_[v];
-                ghost_state(P, -nb, nx, ny, nz, so);
-                // the viscous flux reads the ghost of the cell-centre state (DP/computePrimVec.cu:61-76)
-#pragma unroll
-                for (int v = 0; v < NP; v++) p1[v] = w[v];
-                ghost_state(P, -nb, nx, ny, nz, p1);
-#pragma unroll
-                for (int q = 0; q < 9; q++) gO[q] = gN[q] = g[NP + 9 + q];
-                vAvg = (T)vc;
+            for (int q = 0; q < 9; q++) {
+                const T gc = gO[q];
+                gO[q] = own ? gc : gn[NP + 9 + q];
+                gN[q] = own ? gn[NP + 9 + q] : gc;
             }
-            const T *L = own ? sc_ : so;
-            const T *R = own ? so : sc_;
-            if (nb >= 0) {
+            const double vn = m.vol[nb];
+            vAvg = (T)((own ? (vc + vn) : (vn + vc)) * 0.5);
+        } else {
+            // ghost of the reconstructed state for the flux (DP/computeRHS.cu:113)
 #pragma unroll
-                for (int v = 0; v < NP; v++) p1[v] = R[v];
-            }
-            T F[NV], unc, pF;
-            hllc_flux(P, L, R, nx, ny, nz, F, unc, pF);
-            // side terms with this cell's centre state (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
-            const T sgn = own ? (T)-1 : (T)1;
-            const T dp = pF - pc;
-            T cb[NV];
-            cb[0] = sgn * (F[0] - w[0] * unc) * A;
-            cb[1] = sgn * F[1] * A;
-            cb[2] = sgn * F[2] * A;
-            cb[3] = sgn * (F[3] + dp * nx) * A;
-            cb[4] = sgn * (F[4] + dp * ny) * A;
-            cb[5] = sgn * (F[5] + dp * nz) * A;
-            cb[6] = sgn * (F[6] + w[0] * w[6] * unc) * A;
-            cb[7] = sgn * (F[7] + (1 - w[0]) * w[7] * unc) * A;
-            cb[8] = sgn * F[8] * A;
-            cb[9] = sgn * F[9] * A;
-            if (P.visc) {
-                // DP/computeViscousStresses.cu:87-170 with slot 0 = owner face state (L)
-                T gv[9];
+            for (int v = 0; v < NP; v++) so[v] = sc_[v];
+            ghost_state(P, -nb, nx, ny, nz, so);
+            // the viscous flux reads the ghost of the cell-centre state (DP/computePrimVec.cu:61-76)
 #pragma unroll
-                for (int q = 0; q < 9; q++) gv[q] = (gO[q] + gN[q]) * (T)0.5;
-                const T nut = P.turb ? wale_nu(gv, vAvg) : (T)0;
-                const T dv = (gv[0] + gv[4] + gv[8]) * ((T)2 / 3);
-                const T t00 = 2 * gv[0] - dv, t11 = 2 * gv[4] - dv, t22 = 2 * gv[8] - dv;
-                const T t01 = gv[1] + gv[3], t02 = gv[2] + gv[6], t12 = gv[5] + gv[7];
-                const T a1 = L[0], r1 = L[0] * L[1] + (1 - L[0]) * L[2];
-                const T a2 = p1[0], r2 = p1[0] * p1[1] + (1 - p1[0]) * p1[2];
-                const T mu = (a1 + a2) * (T)0.5 * P.mu[0] + (1 - (a1 + a2) * (T)0.5) * P.mu[1] + (r1 + r2) * (T)0.5 * nut;
-                const T fmx = mu * (t00 * nx + t01 * ny + t02 * nz);
-                const T fmy = mu * (t01 * nx + t11 * ny + t12 * nz);
-                const T fmz = mu * (t02 * nx + t12 * ny + t22 * nz);
-                const T vx = (L[3] + p1[3]) * (T)0.5, vy = (L[4] + p1[4]) * (T)0.5, vz = (L[5] + p1[5]) * (T)0.5;
-                const T fe = mu * ((t00 * vx + t01 * vy + t02 * vz) * nx + (t01 * vx + t11 * vy + t12 * vz) * ny +
-                                   (t02 * vx + t12 * vy + t22 * vz) * nz);
-                const T vs = own ? A : -A;
-                cb[3] += fmx * vs;
-                cb[4] += fmy * vs;
-                cb[5] += fmz * vs;
-                cb[8] += fe * vs;
-            }
+            for (int v = 0; v < NP; v++) p1[v] = w[v];
+            ghost_state(P, -nb, nx, ny, nz, p1);
 #pragma unroll
-            for (int v = 0; v < NV; v++) acc[v] += (double)cb[v];
-            if (wantSignal) {
-                T s = face_signal(P, sc_, nx, ny, nz);
-                if (nb >= 0) s = fmax(s, face_signal(P, so, nx, ny, nz));
-                sig = fmax(sig, s);
-            }
+            for (int q = 0; q < 9; q++) gN[q] = gO[q];
+            vAvg = (T)vc;
+        }
+        const T *L = own ? sc_ : so;
+        const T *R = own ? so : sc_;
+        if (nb >= 0) {
+#pragma unroll
+            for (int v = 0; v < NP; v++) p1[v] = R[v];
+        }
+        T F[NV], unc, pF;
+        hllc_flux(P, L, R, nx, ny, nz, F, unc, pF);
+        // side terms with this cell's centre state (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
+        const T pc = w[0] * w[6] + (1 - w[0]) * w[7];
+        const T sgn = own ? (T)-1 : (T)1;
+        const T dp = pF - pc;
+        cb[0] = sgn * (F[0] - w[0] * unc) * A;
+        cb[1] = sgn * F[1] * A;
+        cb[2] = sgn * F[2] * A;
+        cb[3] = sgn * (F[3] + dp * nx) * A;
+        cb[4] = sgn * (F[4] + dp * ny) * A;
+        cb[5] = sgn * (F[5] + dp * nz) * A;
+        cb[6] = sgn * (F[6] + w[0] * w[6] * unc) * A;
+        cb[7] = sgn * (F[7] + (1 - w[0]) * w[7] * unc) * A;
+        cb[8] = sgn * F[8] * A;
+        cb[9] = sgn * F[9] * A;
+        if (P.visc) {
+            // DP/computeViscousStresses.cu:87-170 with slot 0 = owner face state (L)
+            T gv[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) gv[q] = (gO[q] + gN[q]) * (T)0.5;
+            const T nut = P.turb ? wale_nu(gv, vAvg) : (T)0;
+            const T dv = (gv[0] + gv[4] + gv[8]) * ((T)2 / 3);
+            const T t00 = 2 * gv[0] - dv, t11 = 2 * gv[4] - dv, t22 = 2 * gv[8] - dv;
+            const T t01 = gv[1] + gv[3], t02 = gv[2] + gv[6], t12 = gv[5] + gv[7];
+            const T a1 = L[0], r1 = L[0] * L[1] + (1 - L[0]) * L[2];
+            const T a2 = p1[0], r2 = p1[0] * p1[1] + (1 - p1[0]) * p1[2];
+            const T mu = (a1 + a2) * (T)0.5 * P.mu[0] + (1 - (a1 + a2) * (T)0.5) * P.mu[1] + (r1 + r2) * (T)0.5 * nut;
+            const T fmx = mu * (t00 * nx + t01 * ny + t02 * nz);
+            const T fmy = mu * (t01 * nx + t11 * ny + t12 * nz);
+            const T fmz = mu * (t02 * nx + t12 * ny + t22 * nz);
+            const T vx = (L[3] + p1[3]) * (T)0.5, vy = (L[4] + p1[4]) * (T)0.5, vz = (L[5] + p1[5]) * (T)0.5;
+            const T fe = mu * ((t00 * vx + t01 * vy + t02 * vz) * nx + (t01 * vx + t11 * vy + t12 * vz) * ny +
+                               (t02 * vx + t12 * vy + t22 * vz) * nz);
+            const T vs = own ? A : -A;
+            cb[3] += fmx * vs;
+            cb[4] += fmy * vs;
+            cb[5] += fmz * vs;
+            cb[8] += fe * vs;
         }
         if (wantSignal) {
-            f.signal[c] = (double)sig;
+            sig = face_signal(P, sc_, nx, ny, nz);
+            if (nb >= 0) sig = fmax(sig, face_signal(P, so, nx, ny, nz));
+        }
+    }
+    // cell residual: FP64 butterfly over the group's faces
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) acc[v] = group_sum<G>((double)cb[v]);
+    double cfl = 1e12;   // per-cell CFL bound for the block minimum
+    if (wantSignal) {
+        sig = group_max<G>(sig);
+        if (cell) {
+            if (k == 0) f.signal[c] = (double)sig;
             cfl = m.volP[c] / (double)sig;
         }
-        if (mode == FLUX_RHS) {
+    }
+    if (mode == FLUX_RHS) {
+        // lane j stores variables j, j + G, ...
+        if (cell) {
 #pragma unroll
-            for (int v = 0; v < NV; v++) f.RHS[(size_t)v * n + c] = acc[v];
-        } else {
+            for (int v = 0; v < NV; v++)
+                if (v % G == k) f.RHS[(size_t)v * n + c] = acc[v];
+        }
+    } else {
+        // FP64 Runge-Kutta combination (DP/update.cu:19-103): lane j updates variables j, j + G,
+        // ...; the new state is then shuffled to every lane and lane 0 writes the primitive record
+        double rl[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) rl[v] = 0.0;
+        if (cell) {
             const double dt = *f.dt;
             const double dtv = dt * (1.0 / vc);
-            double u[NV];
 #pragma unroll
             for (int v = 0; v < NV; v++) {
+                if (v % G != k) continue;
                 const size_t q = (size_t)v * n + c;
                 const double uc = f.U[q];
                 double r;
@@ -294,11 +361,16 @@ __global__ void __launch_bounds__(kFluxThreads) k_flux(const DevMesh<T> m, Field
                     r = (1.0 / 3.0) * f.U0[q] + (2.0 / 3.0) * uc + ((2.0 / 3.0) * dt) * (1.0 / vc) * acc[v];
                 }
                 if (v == 5 && sc.neglectZ) r = 0.0;
-                u[v] = r;
                 f.U[q] = r;
+                rl[v] = r;
             }
+        }
+        double un[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) un[v] = __shfl_sync(0xffffffffu, rl[v], v % G, G);
+        if (cell && k == 0) {
             T wo[NP];
-            cons2prim_d(D, u, wo);
+            cons2prim_d(D, un, wo);
             store_rec(f.Wout, c, wo);
         }
     }
@@ -428,17 +500,24 @@ __global__ void k_copy(size_t cnt, const double *__restrict__ a, double *b) {
 }
 
 // ------------------------------------------------------------------ launchers
-int flux_blocks(int n) { return (n + kFluxThreads - 1) / kFluxThreads; }
+int lane_group(int nSlots) { return nSlots <= 4 ? 4 : 8; }
+int flux_blocks(int n, int nSlots) {
+    return (int)(((size_t)n * lane_group(nSlots) + kFluxThreads - 1) / kFluxThreads);
+}
 int cons_blocks(int n) { return (n + kConsThreads - 1) / kConsThreads; }
 
 template <typename T>
 void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cudaStream_t s) {
-    k_grad<T><<<(m.n + kGradThreads - 1) / kGradThreads, kGradThreads, 0, s>>>(m, f.Win, f.G, P);
+    const int nb = (int)(((size_t)m.n * lane_group(m.nSlots) + kGradThreads - 1) / kGradThreads);
+    if (lane_group(m.nSlots) == 4) k_grad<T, 4><<<nb, kGradThreads, 0, s>>>(m, f.Win, f.G, P);
+    else k_grad<T, 8><<<nb, kGradThreads, 0, s>>>(m, f.Win, f.G, P);
 }
 template <typename T>
 void launch_flux(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, const PhysD &D, int mode,
                  int wantSignal, StageCoef sc, cudaStream_t s) {
-    k_flux<T><<<flux_blocks(m.n), kFluxThreads, 0, s>>>(m, f, P, D, mode, wantSignal, sc);
+    const int nb = flux_blocks(m.n, m.nSlots);
+    if (lane_group(m.nSlots) == 4) k_flux<T, 4><<<nb, kFluxThreads, 0, s>>>(m, f, P, D, mode, wantSignal, sc);
+    else k_flux<T, 8><<<nb, kFluxThreads, 0, s>>>(m, f, P, D, mode, wantSignal, sc);
 }
 template <typename T>
 void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, StageCoef sc, cudaStream_t s) {

@@ -4,7 +4,8 @@
 
 namespace fg {
 
-// Cell-ordered (renumbered) device mesh.  Per-slot arrays are slot-major: a[k * n + c].
+// Cell-ordered (renumbered) device mesh.  Per-slot arrays are cell-major: a[c * nSlots + k], so
+// the lanes that work on the faces of one cell read contiguous words.
 template <typename T>
 struct DevMesh {
     int n;              // cells
@@ -51,7 +52,7 @@ template <typename T>
 void launch_prim(int n, const double *U, T *W, const PhysD &D, cudaStream_t s);
 // dt = min(cfl * min_blocks, maxDt) from blockMin[nBlocks]
 void launch_dt_finalize(const double *blockMin, int nBlocks, double cfl, double maxDt, double *dt, cudaStream_t s);
-int flux_blocks(int n);
+int flux_blocks(int n, int nSlots);   // blocks of the flux kernel (= entries of blockMin)
 
 // relaxation (FP64 Newton), writes U and the primitive record
 struct RelaxParams {

@@ -224,7 +224,7 @@ struct SolverT : public fg_solver {
                 const int f = elFc2fc[(size_t)o * 6 + k];
                 const int side = elFcSide[(size_t)o * 6 + k];
                 if (f < 0) return set_err(FG_ERR_MESH, "internal: element face without a face record");
-                const size_t q = (size_t)k * n + i;
+                const size_t q = (size_t)i * nSlots + k;   // cell-major: the lanes of a cell read contiguously
                 const int bc = m.boundCond[f];
                 const int own = m.fc2el[2 * f], nbo = m.fc2el[2 * f + 1];
                 const double *fc = &m.fcCenter[(size_t)f * 3];
@@ -276,7 +276,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dW[1].alloc((size_t)n * WREC * sizeof(T)));
         FG_CUDA_TRY(dG.alloc((size_t)n * GREC * sizeof(T)));
         FG_CUDA_TRY(dSig.alloc((size_t)n * sizeof(double)));
-        FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n), cons_blocks(n)) * sizeof(double)));
+        FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n, nSlots), cons_blocks(n)) * sizeof(double)));
         FG_CUDA_TRY(dScal.alloc(4 * sizeof(double)));   // dt, time, cons
         FG_CUDA_TRY(dCnt.alloc(4 * sizeof(int32_t)));
         FG_CUDA_TRY(cudaMemset(dU.p, 0, u));
@@ -345,7 +345,7 @@ struct SolverT : public fg_solver {
     }
     int time_step(double *dtOut, cudaStream_t s) override {
         prof_begin(FG_K_DT, s);
-        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(n), cs.cfl, cs.maxDt, dScal.as<double>(), s);
+        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(n, nSlots), cs.cfl, cs.maxDt, dScal.as<double>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("time_step");
         if (dtOut) {
