@@ -44,17 +44,19 @@ def _run(cmd, cwd=None):
     return r.stdout + r.stderr
 
 
-def build_product(force: bool = False, verbose: bool = False) -> Path:
+def build_product(force: bool = False, verbose: bool = False, out: Path = None, defines=()) -> Path:
     cu = [CSRC / "fg_kernels.cu", CSRC / "fg_relax.cu", CSRC / "fg_solver.cu"]
     cpp = [CSRC / "fg_mesh.cpp"]
     hdr = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "fooskagpu.h"]
-    if not force and not _stale(LIB, cu + cpp + hdr):
-        return LIB
-    objdir = ROOT / "_build"
-    objdir.mkdir(exist_ok=True)
+    lib_out = out or LIB
+    if not force and not _stale(lib_out, cu + cpp + hdr):
+        return lib_out
+    objdir = ROOT / "_build" / (lib_out.stem if out else "")
+    objdir.mkdir(parents=True, exist_ok=True)
     nvcc = _nvcc()
     objs = []
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-I", str(ROOT / "include")]
+    common += [f"-D{d}" for d in defines]
     for s in cu:
         o = objdir / (s.stem + ".o")
         cmd = [nvcc, *ARCH, "-lineinfo", *common, "-c", str(s), "-o", str(o)]
@@ -72,10 +74,10 @@ def build_product(force: bool = False, verbose: bool = False) -> Path:
         o = objdir / (s.stem + ".o")
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", str(ROOT / "include"), "-c", str(s), "-o", str(o)])
         objs.append(o)
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = lib_out.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"])
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib_out)
+    return lib_out
 
 
 def build_oracle(force: bool = False) -> Path:

@@ -12,12 +12,40 @@ struct DevMesh {
     int nSlots;         // max faces per cell
     const int32_t *nbr;   // neighbour cell, or -bc (1..5) on a boundary slot, or INT32_MIN unused
     const int32_t *flags; // bits 0-2: faces of the cell; bit 3+k: cell owns the face of slot k
+    // the ten per-slot geometry arrays below are consecutive blocks of geoStride values, in this
+    // order, starting at nx; geoStride >= n * nSlots is a multiple of 16 bytes so that every
+    // component starts 16-byte aligned and 16-byte reads of a block's range stay inside it
+    size_t geoStride;
     const T *nx, *ny, *nz, *A;       // canonical (owner -> neighbour) unit normal and area
     const T *dcx, *dcy, *dcz;        // face centre - own cell centre
     const T *dnx, *dny, *dnz;        // face centre - neighbour cell centre (periodic image)
     const double *vol;               // cell volume
     const double *volP;              // pow(vol, 0.3333) as the reference's CFL bound uses
+    // shared-memory staging: blocks of `blockCells` consecutive cells; the face neighbours of a
+    // block that lie outside it (its halo) are listed in haloIds[haloStart[b] .. haloStart[b+1]);
+    // slotLocal[c * nSlots + k] is the neighbour's index in the block's staged records (own cells
+    // first, then the halo), or -bc on a boundary slot.
+    int blockCells;
+    int maxHalo;
+    const int32_t *haloStart;
+    const int32_t *haloIds;
+    const int16_t *slotLocal;
 };
+
+// cells per block of the staged stage kernels (FP32 and FP64 records differ in size)
+#ifndef FG_STAGE_CELLS_F
+#define FG_STAGE_CELLS_F 128
+#endif
+#ifndef FG_STAGE_CELLS_D
+#define FG_STAGE_CELLS_D 64
+#endif
+// 1: the per-slot geometry of a block is staged in shared memory with its records;
+// 0: each face reads its geometry from global memory
+#ifndef FG_STAGE_GEOMETRY
+#define FG_STAGE_GEOMETRY 1
+#endif
+template <typename T> struct StageCells { static constexpr int value = FG_STAGE_CELLS_F; };
+template <> struct StageCells<double> { static constexpr int value = FG_STAGE_CELLS_D; };
 
 template <typename T>
 struct Fields {
@@ -43,6 +71,9 @@ struct StageCoef {
 
 template <typename T>
 void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cudaStream_t s);
+// one-time kernel attribute set-up (dynamic shared memory above 48 KB)
+template <typename T>
+int stage_kernels_setup(const DevMesh<T> &m);
 template <typename T>
 void launch_flux(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, const PhysD &D,
                  int mode, int wantSignal, StageCoef sc, cudaStream_t s);
@@ -52,7 +83,7 @@ template <typename T>
 void launch_prim(int n, const double *U, T *W, const PhysD &D, cudaStream_t s);
 // dt = min(cfl * min_blocks, maxDt) from blockMin[nBlocks]
 void launch_dt_finalize(const double *blockMin, int nBlocks, double cfl, double maxDt, double *dt, cudaStream_t s);
-int flux_blocks(int n, int nSlots);   // blocks of the flux kernel (= entries of blockMin)
+int flux_blocks(int n, int blockCells);   // blocks of the flux kernel (= entries of blockMin)
 
 // relaxation (FP64 Newton), writes U and the primitive record
 struct RelaxParams {

@@ -126,7 +126,7 @@ __global__ void k_advance_time(const double *dt, double *t) { *t += *dt; }
 
 template <typename T>
 struct SolverT : public fg_solver {
-    DevBuf dNbr, dFlags, dGeo, dVol, dVolP, dNew2Old;
+    DevBuf dNbr, dFlags, dGeo, dVol, dVolP, dNew2Old, dHaloStart, dHaloIds, dSlotLocal;
     DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dBlockMin, dScal, dCnt, dCons, dStage;
     int cur = 0;
     DevMesh<T> dm{};
@@ -211,8 +211,10 @@ struct SolverT : public fg_solver {
             }
         }
         const size_t S = (size_t)nSlots * n;
+        // component stride of the geometry arrays: padded to 16 bytes (see DevMesh::geoStride)
+        const size_t GS = (S * sizeof(T) + 15) / 16 * 16 / sizeof(T);
         std::vector<int32_t> nbr(S, INT32_MIN), flags(n, 0);
-        std::vector<T> geo(10 * S, (T)0);
+        std::vector<T> geo(10 * GS, (T)0);
         std::vector<double> volP(n), vol(n);
         for (int i = 0; i < n; i++) {
             const int o = m.new2old[i];
@@ -240,30 +242,81 @@ struct SolverT : public fg_solver {
                 } else {
                     nbr[q] = m.old2new[own];
                 }
-                for (int d = 0; d < 3; d++) geo[(size_t)d * S + q] = (T)m.n[(size_t)f * 3 + d];
-                geo[3 * S + q] = (T)m.area[f];
+                for (int d = 0; d < 3; d++) geo[(size_t)d * GS + q] = (T)m.n[(size_t)f * 3 + d];
+                geo[3 * GS + q] = (T)m.area[f];
                 for (int d = 0; d < 3; d++) {
                     const double dcv = (side == 0) ? xOwnSide[d] - m.cellCenter[(size_t)o * 3 + d]
                                                    : xNbSide[d] - m.cellCenter[(size_t)o * 3 + d];
                     double dnv = 0.0;
                     if (side == 0 && bc == 0) dnv = xNbSide[d] - m.cellCenter[(size_t)nbo * 3 + d];
                     if (side == 1) dnv = xOwnSide[d] - m.cellCenter[(size_t)own * 3 + d];
-                    geo[(size_t)(4 + d) * S + q] = (T)dcv;
-                    geo[(size_t)(7 + d) * S + q] = (T)dnv;
+                    geo[(size_t)(4 + d) * GS + q] = (T)dcv;
+                    geo[(size_t)(7 + d) * GS + q] = (T)dnv;
                 }
             }
             flags[i] = fl;
         }
+        // shared-memory staging plan: per block of B consecutive cells, the list of face
+        // neighbours outside the block and each slot's index among the staged records
+        const int B = StageCells<T>::value;
+        const int nBlk = (n + B - 1) / B;
+        std::vector<int32_t> haloStart(nBlk + 1, 0), haloIds;
+        std::vector<int16_t> slotLocal(S, -1);
+        haloIds.reserve((size_t)n * 2);
+        int maxHalo = 0;
+        {
+            std::vector<int32_t> stamp(n, -1), pos(n, 0);
+            for (int b = 0; b < nBlk; b++) {
+                const int lo = b * B, hi = std::min(n, lo + B);
+                int H = 0;
+                for (int i = lo; i < hi; i++) {
+                    const int nfc = flags[i] & 7;
+                    for (int k = 0; k < nfc; k++) {
+                        const size_t q = (size_t)i * nSlots + k;
+                        const int nb = nbr[q];
+                        if (nb < 0) {
+                            slotLocal[q] = (int16_t)nb;   // -bc
+                            continue;
+                        }
+                        if (nb >= lo && nb < hi) {
+                            slotLocal[q] = (int16_t)(nb - lo);
+                        } else {
+                            if (stamp[nb] != b) {
+                                stamp[nb] = b;
+                                pos[nb] = H++;
+                                haloIds.push_back(nb);
+                            }
+                            if (B + pos[nb] > 32767) return set_err(FG_ERR_MESH, "staging halo too large");
+                            slotLocal[q] = (int16_t)(B + pos[nb]);
+                        }
+                    }
+                }
+                haloStart[b + 1] = (int32_t)haloIds.size();
+                maxHalo = std::max(maxHalo, H);
+            }
+        }
         FG_CUDA_TRY(cudaSetDevice(device));
+        FG_CUDA_TRY(dHaloStart.alloc((size_t)(nBlk + 1) * sizeof(int32_t)));
+        FG_CUDA_TRY(dHaloIds.alloc(std::max<size_t>(haloIds.size(), 1) * sizeof(int32_t)));
+        FG_CUDA_TRY(dSlotLocal.alloc(S * sizeof(int16_t)));
+        FG_CUDA_TRY(cudaMemcpy(dHaloStart.p, haloStart.data(), haloStart.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        if (!haloIds.empty())
+            FG_CUDA_TRY(cudaMemcpy(dHaloIds.p, haloIds.data(), haloIds.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dSlotLocal.p, slotLocal.data(), S * sizeof(int16_t), cudaMemcpyHostToDevice));
+        dm.blockCells = B;
+        dm.maxHalo = maxHalo;
+        dm.haloStart = dHaloStart.as<int32_t>();
+        dm.haloIds = dHaloIds.as<int32_t>();
+        dm.slotLocal = dSlotLocal.as<int16_t>();
         FG_CUDA_TRY(dNbr.alloc(S * sizeof(int32_t)));
         FG_CUDA_TRY(dFlags.alloc((size_t)n * sizeof(int32_t)));
-        FG_CUDA_TRY(dGeo.alloc(10 * S * sizeof(T)));
+        FG_CUDA_TRY(dGeo.alloc(10 * GS * sizeof(T)));
         FG_CUDA_TRY(dVol.alloc((size_t)n * sizeof(double)));
         FG_CUDA_TRY(dVolP.alloc((size_t)n * sizeof(double)));
         FG_CUDA_TRY(dNew2Old.alloc((size_t)n * sizeof(int32_t)));
         FG_CUDA_TRY(cudaMemcpy(dNbr.p, nbr.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dFlags.p, flags.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
-        FG_CUDA_TRY(cudaMemcpy(dGeo.p, geo.data(), 10 * S * sizeof(T), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dGeo.p, geo.data(), 10 * GS * sizeof(T), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dVol.p, vol.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dVolP.p, volP.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dNew2Old.p, m.new2old.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
@@ -276,7 +329,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dW[1].alloc((size_t)n * WREC * sizeof(T)));
         FG_CUDA_TRY(dG.alloc((size_t)n * GREC * sizeof(T)));
         FG_CUDA_TRY(dSig.alloc((size_t)n * sizeof(double)));
-        FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n, nSlots), cons_blocks(n)) * sizeof(double)));
+        FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n, StageCells<T>::value), cons_blocks(n)) * sizeof(double)));
         FG_CUDA_TRY(dScal.alloc(4 * sizeof(double)));   // dt, time, cons
         FG_CUDA_TRY(dCnt.alloc(4 * sizeof(int32_t)));
         FG_CUDA_TRY(cudaMemset(dU.p, 0, u));
@@ -289,18 +342,22 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(cudaMemcpy(dScal.p, scal, sizeof(scal), cudaMemcpyHostToDevice));
         bytes = 0;
         for (DevBuf *b : {&dNbr, &dFlags, &dGeo, &dVol, &dVolP, &dNew2Old, &dU, &dU0, &dRHS, &dStage, &dW[0], &dW[1], &dG,
-                          &dSig, &dBlockMin, &dScal, &dCnt})
+                          &dSig, &dBlockMin, &dScal, &dCnt, &dHaloStart, &dHaloIds, &dSlotLocal})
             bytes += b->bytes;
         dm.n = n;
         dm.nSlots = nSlots;
         dm.nbr = dNbr.as<int32_t>();
         dm.flags = dFlags.as<int32_t>();
         T *g = dGeo.as<T>();
-        dm.nx = g + 0 * S; dm.ny = g + 1 * S; dm.nz = g + 2 * S; dm.A = g + 3 * S;
-        dm.dcx = g + 4 * S; dm.dcy = g + 5 * S; dm.dcz = g + 6 * S;
-        dm.dnx = g + 7 * S; dm.dny = g + 8 * S; dm.dnz = g + 9 * S;
+        dm.geoStride = GS;
+        dm.nx = g + 0 * GS; dm.ny = g + 1 * GS; dm.nz = g + 2 * GS; dm.A = g + 3 * GS;
+        dm.dcx = g + 4 * GS; dm.dcy = g + 5 * GS; dm.dcz = g + 6 * GS;
+        dm.dnx = g + 7 * GS; dm.dny = g + 8 * GS; dm.dnz = g + 9 * GS;
         dm.vol = dVol.as<double>();
         dm.volP = dVolP.as<double>();
+        if (stage_kernels_setup<T>(dm) != 0)
+            return set_err(FG_ERR_CUDA, "stage kernels need more shared memory than the device allows (halo " +
+                                            std::to_string(maxHalo) + " cells)");
         return FG_OK;
     }
 
@@ -345,7 +402,7 @@ struct SolverT : public fg_solver {
     }
     int time_step(double *dtOut, cudaStream_t s) override {
         prof_begin(FG_K_DT, s);
-        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(n, nSlots), cs.cfl, cs.maxDt, dScal.as<double>(), s);
+        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(n, StageCells<T>::value), cs.cfl, cs.maxDt, dScal.as<double>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("time_step");
         if (dtOut) {
