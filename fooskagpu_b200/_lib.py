@@ -59,7 +59,7 @@ class FgKernelTimes(C.Structure):
     _fields_ = [("ms", f64 * 8), ("launches", C.c_int64 * 8)]
 
 
-KERNEL_KINDS = ["grad", "flux", "update", "relax", "dt", "cons", "other", "unused"]
+KERNEL_KINDS = ["grad", "flux", "update", "relax", "dt", "cons", "other", "gather"]
 
 
 class FgRelaxStats(C.Structure):

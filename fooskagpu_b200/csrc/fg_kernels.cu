@@ -1,19 +1,18 @@
 // Kernels of the per-stage residual path (sm_100a).
 //
-// Dataflow per Runge-Kutta stage (no atomics, no face buffers):
-//   k_grad : cell-centric.  Primitive states of the cell and its face neighbours (or boundary
-//            ghosts) -> Green-Gauss gradient, neighbour min/max, limiter theta.
-//            Replaces convert2PrimVec + greenGauss + computeLimiter
-//            (DP/computePrimVec.cu:38, DP/computeGrad.cu:158, DP/computeFaceValues.cu:29).
-//   k_flux : cell-centric.  For every face of the cell: MUSCL face states of both sides,
-//            HLLC + non-conservative terms + pressure correction, WALE + viscous flux;
-//            the cell's residual is summed in registers (deterministic owner-side gather),
-//            then the FP64 Runge-Kutta combination and the new primitive record.
-//            Replaces updateFaces + computeFlux + computeViscousStresses + rk3stage*/rungeKutta
-//            (DP/computeFaceValues.cu:91, DP/computeRHS.cu:78, DP/computeViscousStresses.cu:66,
-//            DP/update.cu:19-103).
-// Both cells of an interior face evaluate its flux from identical inputs in the canonical
-// (owner -> neighbour) orientation, so owner and neighbour contributions cancel exactly.
+// Dataflow per Runge-Kutta stage (no atomics):
+//   k_grad   : cell-centric.  Primitive states of the cell and its face neighbours (or boundary
+//              ghosts) -> Green-Gauss gradient, neighbour min/max, limiter theta.
+//              Replaces convert2PrimVec + greenGauss + computeLimiter
+//              (DP/computePrimVec.cu:38, DP/computeGrad.cu:158, DP/computeFaceValues.cu:29).
+//   k_face   : one thread per face.  MUSCL face states of both sides, HLLC flux with the
+//              non-conservative and pressure terms, WALE + viscous flux, written once as a
+//              12-word face record.  Replaces updateFaces + computeFlux + computeViscousStresses
+//              (DP/computeFaceValues.cu:91, DP/computeRHS.cu:78, DP/computeViscousStresses.cu:66).
+//   k_gather : one thread per cell.  Sums the records of the cell's faces with its orientation
+//              sign in FP64 in slot order (deterministic owner-side gather), adds the cell-centre
+//              terms, then the FP64 Runge-Kutta combination and the new primitive record
+//              (DP/update.cu:19-103), or stores the residual.
 #include "fg_kernels.cuh"
 
 #include <climits>
@@ -78,6 +77,34 @@ __device__ __forceinline__ void store_g<float>(float *G, int c, const float *g) 
     for (int q = 0; q < GREC / 4; q++) p[q] = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
 }
 
+template <typename T>
+__device__ __forceinline__ void store_frec(T *FB, int f, const T *r) {
+    T *p = FB + (size_t)f * FREC;
+#pragma unroll
+    for (int v = 0; v < FREC; v++) p[v] = r[v];
+}
+template <>
+__device__ __forceinline__ void store_frec<float>(float *FB, int f, const float *r) {
+    float4 *p = reinterpret_cast<float4 *>(FB + (size_t)f * FREC);
+    p[0] = make_float4(r[0], r[1], r[2], r[3]);
+    p[1] = make_float4(r[4], r[5], r[6], r[7]);
+    p[2] = make_float4(r[8], r[9], r[10], r[11]);
+}
+template <typename T>
+__device__ __forceinline__ void load_frec(const T *__restrict__ FB, int f, T *r) {
+    const T *p = FB + (size_t)f * FREC;
+#pragma unroll
+    for (int v = 0; v < FREC; v++) r[v] = __ldg(p + v);
+}
+template <>
+__device__ __forceinline__ void load_frec<float>(const float *__restrict__ FB, int f, float *r) {
+    const float4 *p = reinterpret_cast<const float4 *>(FB + (size_t)f * FREC);
+    const float4 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2);
+    r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
+    r[4] = b.x; r[5] = b.y; r[6] = b.z; r[7] = b.w;
+    r[8] = d.x; r[9] = d.y; r[10] = d.z; r[11] = d.w;
+}
+
 // ------------------------------------------------------------------ shared-memory staging
 // A block handles `blockCells` consecutive (Morton-ordered, hence spatially compact) cells.  It
 // first copies into shared memory
@@ -101,17 +128,10 @@ __host__ __device__ inline size_t rec_area(const DevMesh<T> &m, int stride) {
 template <typename T> struct Stage;
 template <> struct Stage<float> {
     static constexpr int WS = 13;   // W(9) + volume + pad, odd
-    static constexpr int RS = 47;   // W(9) theta(9) grad(27) volume + pad, odd
 };
 template <> struct Stage<double> {
     static constexpr int WS = 11;
-    static constexpr int RS = 47;
 };
-// staged record layout (in T): [0..8] W, [9] volume, then (flux records) [10..18] theta,
-// [19..45] grad
-constexpr int kRecVol = 9;
-constexpr int kRecTh = 10;
-constexpr int kRecGrad = 19;
 __host__ __device__ constexpr int slot_stride(int nSlots) { return nSlots | 1; }
 
 // per-slot geometry of a cell: staged in shared memory, or read from global memory
@@ -278,166 +298,143 @@ __global__ void __launch_bounds__(StageCells<T>::value) k_grad(const DevMesh<T> 
     store_g(G, c, out);
 }
 
-// MUSCL face state of a cell: w + theta * ((x_f - x_c) . grad w)  (DP/computeFaceValues.cu:66-105);
-// r points at a staged record
+// MUSCL face state of a cell: w + theta * ((x_f - x_c) . grad w)  (DP/computeFaceValues.cu:66-105)
 template <typename T>
-__device__ __forceinline__ void face_state(const T *r, T dx, T dy, T dz, T *s) {
+__device__ __forceinline__ void face_state(const T *w, const T *g, T dx, T dy, T dz, T *s) {
 #pragma unroll
     for (int v = 0; v < NP; v++) {
-        const T *g = r + kRecGrad + 3 * v;
-        const T ext = fma(dx, g[0], fma(dy, g[1], dz * g[2]));
-        s[v] = fma(r[kRecTh + v], ext, r[v]);
+        const T ext = fma(dx, g[NP + 3 * v], fma(dy, g[NP + 3 * v + 1], dz * g[NP + 3 * v + 2]));
+        s[v] = fma(g[v], ext, w[v]);
     }
 }
 
-// ------------------------------------------------------------------ flux + gather + RK
+// ------------------------------------------------------------------ face flux (once per face)
+// Record of face f with canonical normal n (owner -> neighbour), area A:
+//   H[v] = A (F[v] - Visc[v]) + A pF n (momentum),  u = A (u* . n),  signal
+// where F is the HLLC + advective flux (DP/computeRHS.cu:117-131), Visc the WALE viscous flux
+// (DP/computeViscousStresses.cu:87-170) and pF the upwind mixture pressure.  A cell with
+// orientation s (-1 owner, +1 neighbour, the reference's sign) receives s * H[v] plus its
+// cell-centre terms, which k_gather adds from sums over its faces:
+//   var 0: -alpha_c s u,  vars 6/7: +alpha_c pL_c s u, +(1-alpha_c) pG_c s u,
+//   momentum: -pC_c s A n summed = pC_c * (sum of outward n A)  (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
 template <typename T>
-__global__ void __launch_bounds__(StageCells<T>::value) k_flux(const DevMesh<T> m, Fields<T> f, const PhysT<T> P,
-                                                                const PhysD D, int mode, int wantSignal, StageCoef sc) {
-    constexpr int RS = Stage<T>::RS;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int b = blockIdx.x;
-    const int B = m.blockCells;
-    const int lo = b * B;
-    const int n = m.n;
-    const int nOwn = min(B, n - lo);
-    const int nRec = B + (m.haloStart[b + 1] - m.haloStart[b]);
-    const int SS = slot_stride(m.nSlots);
-    T *rec = reinterpret_cast<T *>(smem_raw);
-    T *sg = reinterpret_cast<T *>(smem_raw + rec_area<T>(m, RS));
-    int *sl = reinterpret_cast<int *>(sg + (size_t)kGeoComp * B * m.nSlots);
-    // records: W(9) | volume | theta(9) grad(27): 16-byte vectors of the W and G records, the
-    // volume taken by the lane that copies the W vector holding W[8]
+__global__ void __launch_bounds__(128) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
+                                              T *__restrict__ FB, const PhysT<T> P, int wantSignal) {
+    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fi >= m.nF) return;
+    const int o = m.fOwn[fi];
+    const int nb = m.fNb[fi];
+    const T nx = m.fnx[fi], ny = m.fny[fi], nz = m.fnz[fi], A = m.fA[fi];
+    T wo[NP], sL[NP], sR[NP], p1[NP], gO[9], gN[9];
     {
-        using V = typename Vec16<T>::type;
-        constexpr int TPV = 16 / sizeof(T);
-        constexpr int WV = WREC / TPV, GV = GREC / TPV, NVR = WV + GV;
-        const V *Wv = reinterpret_cast<const V *>(f.Win);
-        const V *Gv = reinterpret_cast<const V *>(f.G);
-        for (int i = threadIdx.x; i < nRec * NVR; i += blockDim.x) {
-            const int r = i / NVR, q = i - (i / NVR) * NVR;
-            const int src = staged_source(m, b, r, lo, nOwn);
-            if (src < 0) continue;
-            T *dst = rec + r * RS;
-            if (q < WV) {
-                const V x = __ldg(Wv + (size_t)src * WV + q);
-                const T *xs = reinterpret_cast<const T *>(&x);
+        T g[GREC];
+        load_rec(W, o, wo);
+        load_g(G, o, g);
+        face_state(wo, g, m.fdo[0][fi], m.fdo[1][fi], m.fdo[2][fi], sL);
 #pragma unroll
-                for (int j = 0; j < TPV; j++)
-                    if (q * TPV + j < NP) dst[q * TPV + j] = xs[j];
-                if (q * TPV <= NP - 1 && NP - 1 < (q + 1) * TPV) dst[kRecVol] = (T)m.vol[src];
-            } else {
-                const V x = __ldg(Gv + (size_t)src * GV + (q - WV));
-                const T *xs = reinterpret_cast<const T *>(&x);
-#pragma unroll
-                for (int j = 0; j < TPV; j++) dst[kRecTh + (q - WV) * TPV + j] = xs[j];
-            }
-        }
+        for (int q = 0; q < 9; q++) gO[q] = g[NP + 9 + q];
     }
-    stage_geometry(m, lo, nOwn, sg, sl);
-    __syncthreads();
-    const int t = threadIdx.x;
-    const int c = lo + t;
-    const bool cell = t < nOwn;
-    const SlotGeo<T> geo{sg, sl, B * m.nSlots, t * m.nSlots, &m, (size_t)c * m.nSlots};
-    double cfl = 1e12;   // per-cell CFL bound for the block minimum
-    if (cell) {
-        const T *me = rec + t * RS;
-        T w[NP];
+    if (nb >= 0) {
+        T wn[NP], g[GREC];
+        load_rec(W, nb, wn);
+        load_g(G, nb, g);
+        face_state(wn, g, m.fdn[0][fi], m.fdn[1][fi], m.fdn[2][fi], sR);
 #pragma unroll
-        for (int v = 0; v < NP; v++) w[v] = me[v];
-        const T pc = w[0] * w[6] + (1 - w[0]) * w[7];
-        double acc[NV];
+        for (int q = 0; q < 9; q++) gN[q] = g[NP + 9 + q];
+#pragma unroll
+        for (int v = 0; v < NP; v++) p1[v] = sR[v];
+    } else {
+        // ghost of the reconstructed state for the flux (DP/computeRHS.cu:113); the viscous flux
+        // reads the ghost of the cell-centre state (DP/computePrimVec.cu:61-76) and the owner's
+        // gradient twice
+#pragma unroll
+        for (int v = 0; v < NP; v++) {
+            sR[v] = sL[v];
+            p1[v] = wo[v];
+        }
+        ghost_state(P, -nb, nx, ny, nz, sR);
+        ghost_state(P, -nb, nx, ny, nz, p1);
+#pragma unroll
+        for (int q = 0; q < 9; q++) gN[q] = gO[q];
+    }
+    T F[NV], unc, pF;
+    hllc_flux(P, sL, sR, nx, ny, nz, F, unc, pF);
+    T H[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) H[v] = A * F[v];
+    H[3] += A * pF * nx;
+    H[4] += A * pF * ny;
+    H[5] += A * pF * nz;
+    if (P.visc) {
+        T gv[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++) gv[q] = (gO[q] + gN[q]) * (T)0.5;
+        const T nut = P.turb ? wale_nu(gv, m.fVavg[fi]) : (T)0;
+        const T dv = (gv[0] + gv[4] + gv[8]) * ((T)2 / 3);
+        const T t00 = 2 * gv[0] - dv, t11 = 2 * gv[4] - dv, t22 = 2 * gv[8] - dv;
+        const T t01 = gv[1] + gv[3], t02 = gv[2] + gv[6], t12 = gv[5] + gv[7];
+        const T a1 = sL[0], r1 = sL[0] * sL[1] + (1 - sL[0]) * sL[2];
+        const T a2 = p1[0], r2 = p1[0] * p1[1] + (1 - p1[0]) * p1[2];
+        const T mu = (a1 + a2) * (T)0.5 * P.mu[0] + (1 - (a1 + a2) * (T)0.5) * P.mu[1] + (r1 + r2) * (T)0.5 * nut;
+        const T vx = (sL[3] + p1[3]) * (T)0.5, vy = (sL[4] + p1[4]) * (T)0.5, vz = (sL[5] + p1[5]) * (T)0.5;
+        const T muA = mu * A;
+        H[3] -= muA * (t00 * nx + t01 * ny + t02 * nz);
+        H[4] -= muA * (t01 * nx + t11 * ny + t12 * nz);
+        H[5] -= muA * (t02 * nx + t12 * ny + t22 * nz);
+        H[8] -= muA * ((t00 * vx + t01 * vy + t02 * vz) * nx + (t01 * vx + t11 * vy + t12 * vz) * ny +
+                       (t02 * vx + t12 * vy + t22 * vz) * nz);
+    }
+    T sig = 0;
+    if (wantSignal) {
+        // DP/computeTimeStep.cu:97-129: both reconstructed sides of an interior face, the owner
+        // side only on a boundary
+        sig = face_signal(P, sL, nx, ny, nz);
+        if (nb >= 0) sig = fmax(sig, face_signal(P, sR, nx, ny, nz));
+    }
+    T rec[FREC];
+#pragma unroll
+    for (int v = 0; v < NV; v++) rec[v] = H[v];
+    rec[NV] = A * unc;
+    rec[NV + 1] = sig;
+    store_frec(FB, fi, rec);
+}
+
+// ------------------------------------------------------------------ owner-side gather + RK
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather(const DevMesh<T> m, Fields<T> f, const PhysD D, int mode,
+                                                int wantSignal, StageCoef sc) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = m.n;
+    double cfl = 1e12;
+    if (c < n) {
+        const int fl = m.flags[c];
+        const int nf = fl & 7;
+        double acc[NV], su = 0.0;
 #pragma unroll
         for (int v = 0; v < NV; v++) acc[v] = 0.0;
         T sig = (T)-1e9;
-        const int fl = m.flags[c];
-        const int nf = fl & 7;
-        const double vc = m.vol[c];
+        const size_t base = (size_t)c * m.nSlots;
         for (int k = 0; k < nf; k++) {
-            const int li = geo.local(k);
-            const bool own = (fl >> (3 + k)) & 1;
-            const T nx = geo.get(0, k), ny = geo.get(1, k), nz = geo.get(2, k), A = geo.get(3, k);
-            T sc_[NP], so[NP];   // own and other reconstructed face states
-            face_state(me, geo.get(4, k), geo.get(5, k), geo.get(6, k), sc_);
-            const T *gme = me + kRecGrad + 9;    // own velocity gradient
-            const T *gO, *gN;                    // velocity gradients of owner / neighbour (viscous)
-            T p1[NP];                            // slot-1 state as the viscous kernel reads it
-            T vAvg;
-            if (li >= 0) {
-                const T *ot = rec + li * RS;
-                face_state(ot, geo.get(7, k), geo.get(8, k), geo.get(9, k), so);
-                const T *gnb = ot + kRecGrad + 9;
-                gO = own ? gme : gnb;
-                gN = own ? gnb : gme;
-                const T vn = ot[kRecVol], vm = me[kRecVol];
-                vAvg = (own ? (vm + vn) : (vn + vm)) * (T)0.5;
-            } else {
-                // ghost of the reconstructed state for the flux (DP/computeRHS.cu:113)
+            const int fi = m.slotFace[base + k];
+            const double s = ((fl >> (3 + k)) & 1) ? -1.0 : 1.0;
+            T rec[FREC];
+            load_frec(f.FB, fi, rec);
 #pragma unroll
-                for (int v = 0; v < NP; v++) so[v] = sc_[v];
-                ghost_state(P, -li, nx, ny, nz, so);
-                // the viscous flux reads the ghost of the cell-centre state (DP/computePrimVec.cu:61-76)
-#pragma unroll
-                for (int v = 0; v < NP; v++) p1[v] = w[v];
-                ghost_state(P, -li, nx, ny, nz, p1);
-                gO = gN = gme;
-                vAvg = me[kRecVol];
-            }
-            const T *L = own ? sc_ : so;
-            const T *R = own ? so : sc_;
-            if (li >= 0) {
-#pragma unroll
-                for (int v = 0; v < NP; v++) p1[v] = R[v];
-            }
-            T F[NV], unc, pF;
-            hllc_flux(P, L, R, nx, ny, nz, F, unc, pF);
-            // side terms with this cell's centre state (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
-            const T sgn = own ? (T)-1 : (T)1;
-            const T dp = pF - pc;
-            T cb[NV];
-            cb[0] = sgn * (F[0] - w[0] * unc) * A;
-            cb[1] = sgn * F[1] * A;
-            cb[2] = sgn * F[2] * A;
-            cb[3] = sgn * (F[3] + dp * nx) * A;
-            cb[4] = sgn * (F[4] + dp * ny) * A;
-            cb[5] = sgn * (F[5] + dp * nz) * A;
-            cb[6] = sgn * (F[6] + w[0] * w[6] * unc) * A;
-            cb[7] = sgn * (F[7] + (1 - w[0]) * w[7] * unc) * A;
-            cb[8] = sgn * F[8] * A;
-            cb[9] = sgn * F[9] * A;
-            if (P.visc) {
-                // DP/computeViscousStresses.cu:87-170 with slot 0 = owner face state (L)
-                T gv[9];
-#pragma unroll
-                for (int q = 0; q < 9; q++) gv[q] = (gO[q] + gN[q]) * (T)0.5;
-                const T nut = P.turb ? wale_nu(gv, vAvg) : (T)0;
-                const T dv = (gv[0] + gv[4] + gv[8]) * ((T)2 / 3);
-                const T t00 = 2 * gv[0] - dv, t11 = 2 * gv[4] - dv, t22 = 2 * gv[8] - dv;
-                const T t01 = gv[1] + gv[3], t02 = gv[2] + gv[6], t12 = gv[5] + gv[7];
-                const T a1 = L[0], r1 = L[0] * L[1] + (1 - L[0]) * L[2];
-                const T a2 = p1[0], r2 = p1[0] * p1[1] + (1 - p1[0]) * p1[2];
-                const T mu = (a1 + a2) * (T)0.5 * P.mu[0] + (1 - (a1 + a2) * (T)0.5) * P.mu[1] + (r1 + r2) * (T)0.5 * nut;
-                const T fmx = mu * (t00 * nx + t01 * ny + t02 * nz);
-                const T fmy = mu * (t01 * nx + t11 * ny + t12 * nz);
-                const T fmz = mu * (t02 * nx + t12 * ny + t22 * nz);
-                const T vx = (L[3] + p1[3]) * (T)0.5, vy = (L[4] + p1[4]) * (T)0.5, vz = (L[5] + p1[5]) * (T)0.5;
-                const T fe = mu * ((t00 * vx + t01 * vy + t02 * vz) * nx + (t01 * vx + t11 * vy + t12 * vz) * ny +
-                                   (t02 * vx + t12 * vy + t22 * vz) * nz);
-                const T vs = own ? A : -A;
-                cb[3] += fmx * vs;
-                cb[4] += fmy * vs;
-                cb[5] += fmz * vs;
-                cb[8] += fe * vs;
-            }
-#pragma unroll
-            for (int v = 0; v < NV; v++) acc[v] += (double)cb[v];
-            if (wantSignal) {
-                T s = face_signal(P, sc_, nx, ny, nz);
-                if (li >= 0) s = fmax(s, face_signal(P, so, nx, ny, nz));
-                sig = fmax(sig, s);
-            }
+            for (int v = 0; v < NV; v++) acc[v] += s * (double)rec[v];
+            su += s * (double)rec[NV];
+            sig = fmax(sig, rec[NV + 1]);
         }
+        T w[NP];
+        load_rec(f.Win, c, w);
+        const double a = w[0], pl = w[6], pg = w[7];
+        const double pc = (double)(w[0] * w[6] + (1 - w[0]) * w[7]);
+        acc[0] -= a * su;
+        acc[6] += a * pl * su;
+        acc[7] += (1.0 - a) * pg * su;
+        acc[3] += pc * (double)m.closure[c];
+        acc[4] += pc * (double)m.closure[(size_t)n + c];
+        acc[5] += pc * (double)m.closure[2 * (size_t)n + c];
+        const double vc = m.vol[c];
         if (wantSignal) {
             f.signal[c] = (double)sig;
             cfl = m.volP[c] / (double)sig;
@@ -601,7 +598,8 @@ __global__ void k_copy(size_t cnt, const double *__restrict__ a, double *b) {
 }
 
 // ------------------------------------------------------------------ launchers
-int flux_blocks(int n, int blockCells) { return (n + blockCells - 1) / blockCells; }
+constexpr int kGatherThreads = 256;
+int flux_blocks(int n) { return (n + kGatherThreads - 1) / kGatherThreads; }
 int cons_blocks(int n) { return (n + kConsThreads - 1) / kConsThreads; }
 
 template <typename T>
@@ -615,14 +613,8 @@ static size_t grad_smem(const DevMesh<T> &m) {
     return rec_area<T>(m, Stage<T>::WS) + geo_smem(m);
 }
 template <typename T>
-static size_t flux_smem(const DevMesh<T> &m) {
-    return rec_area<T>(m, Stage<T>::RS) + geo_smem(m);
-}
-template <typename T>
 int stage_kernels_setup(const DevMesh<T> &m) {
     if (cudaFuncSetAttribute(k_grad<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem(m)) != cudaSuccess)
-        return 1;
-    if (cudaFuncSetAttribute(k_flux<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flux_smem(m)) != cudaSuccess)
         return 1;
     return 0;
 }
@@ -632,10 +624,13 @@ void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cud
     k_grad<T><<<nb, m.blockCells, grad_smem(m), s>>>(m, f.Win, f.G, P);
 }
 template <typename T>
-void launch_flux(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, const PhysD &D, int mode,
-                 int wantSignal, StageCoef sc, cudaStream_t s) {
-    const int nb = (m.n + m.blockCells - 1) / m.blockCells;
-    k_flux<T><<<nb, m.blockCells, flux_smem(m), s>>>(m, f, P, D, mode, wantSignal, sc);
+void launch_face(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, int wantSignal, cudaStream_t s) {
+    k_face<T><<<(m.nF + 127) / 128, 128, 0, s>>>(m, f.Win, f.G, f.FB, P, wantSignal);
+}
+template <typename T>
+void launch_gather(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, int mode, int wantSignal,
+                   StageCoef sc, cudaStream_t s) {
+    k_gather<T><<<flux_blocks(m.n), kGatherThreads, 0, s>>>(m, f, D, mode, wantSignal, sc);
 }
 template int stage_kernels_setup<float>(const DevMesh<float> &);
 template int stage_kernels_setup<double>(const DevMesh<double> &);
@@ -668,8 +663,10 @@ void launch_copy_u0(int n, const double *U, double *U0, cudaStream_t s) {
 
 template void launch_grad<float>(const DevMesh<float> &, const Fields<float> &, const PhysT<float> &, cudaStream_t);
 template void launch_grad<double>(const DevMesh<double> &, const Fields<double> &, const PhysT<double> &, cudaStream_t);
-template void launch_flux<float>(const DevMesh<float> &, const Fields<float> &, const PhysT<float> &, const PhysD &, int, int, StageCoef, cudaStream_t);
-template void launch_flux<double>(const DevMesh<double> &, const Fields<double> &, const PhysT<double> &, const PhysD &, int, int, StageCoef, cudaStream_t);
+template void launch_face<float>(const DevMesh<float> &, const Fields<float> &, const PhysT<float> &, int, cudaStream_t);
+template void launch_face<double>(const DevMesh<double> &, const Fields<double> &, const PhysT<double> &, int, cudaStream_t);
+template void launch_gather<float>(const DevMesh<float> &, const Fields<float> &, const PhysD &, int, int, StageCoef, cudaStream_t);
+template void launch_gather<double>(const DevMesh<double> &, const Fields<double> &, const PhysD &, int, int, StageCoef, cudaStream_t);
 template void launch_update<float>(const DevMesh<float> &, const Fields<float> &, const PhysD &, StageCoef, cudaStream_t);
 template void launch_update<double>(const DevMesh<double> &, const Fields<double> &, const PhysD &, StageCoef, cudaStream_t);
 template void launch_prim<float>(int, const double *, float *, const PhysD &, cudaStream_t);

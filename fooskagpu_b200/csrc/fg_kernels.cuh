@@ -30,7 +30,21 @@ struct DevMesh {
     const int32_t *haloStart;
     const int32_t *haloIds;
     const int16_t *slotLocal;
+    // ---- faces (each evaluated once by k_face), ordered by owner cell, then owner slot ----
+    int nF;
+    size_t fStride;                  // component stride of the face geometry arrays
+    const int32_t *fOwn;             // owner cell
+    const int32_t *fNb;              // neighbour cell, or -bc on a boundary face
+    const T *fnx, *fny, *fnz, *fA;   // canonical unit normal (owner -> neighbour) and area
+    const T *fdo[3];                 // face centre - owner centre
+    const T *fdn[3];                 // face centre - neighbour centre (periodic image)
+    const T *fVavg;                  // (V_owner + V_neighbour) / 2, V_owner on a boundary face
+    const int32_t *slotFace;         // [c * nSlots + k] face of a cell slot
+    const T *closure;                // [3][n] sum over the cell's faces of outward n * A
 };
+
+// face record written by k_face and gathered by k_gather: H[10], u, signal
+constexpr int FREC = 12;
 
 // cells per block of the staged stage kernels (FP32 and FP64 records differ in size)
 #ifndef FG_STAGE_CELLS_F
@@ -42,13 +56,14 @@ struct DevMesh {
 // 1: the per-slot geometry of a block is staged in shared memory with its records;
 // 0: each face reads its geometry from global memory
 #ifndef FG_STAGE_GEOMETRY
-#define FG_STAGE_GEOMETRY 1
+#define FG_STAGE_GEOMETRY 0
 #endif
 template <typename T> struct StageCells { static constexpr int value = FG_STAGE_CELLS_F; };
 template <> struct StageCells<double> { static constexpr int value = FG_STAGE_CELLS_D; };
 
 template <typename T>
 struct Fields {
+    T *FB;              // [nF][FREC] face records
     double *U;          // [10][n]
     double *U0;         // [10][n]
     double *RHS;        // [10][n] (RHS-mode residual)
@@ -75,15 +90,17 @@ void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cud
 template <typename T>
 int stage_kernels_setup(const DevMesh<T> &m);
 template <typename T>
-void launch_flux(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, const PhysD &D,
-                 int mode, int wantSignal, StageCoef sc, cudaStream_t s);
+void launch_face(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, int wantSignal, cudaStream_t s);
+template <typename T>
+void launch_gather(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, int mode, int wantSignal,
+                   StageCoef sc, cudaStream_t s);
 template <typename T>
 void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, StageCoef sc, cudaStream_t s);
 template <typename T>
 void launch_prim(int n, const double *U, T *W, const PhysD &D, cudaStream_t s);
 // dt = min(cfl * min_blocks, maxDt) from blockMin[nBlocks]
 void launch_dt_finalize(const double *blockMin, int nBlocks, double cfl, double maxDt, double *dt, cudaStream_t s);
-int flux_blocks(int n, int blockCells);   // blocks of the flux kernel (= entries of blockMin)
+int flux_blocks(int n);   // blocks of the gather kernel (= entries of blockMin)
 
 // relaxation (FP64 Newton), writes U and the primitive record
 struct RelaxParams {

@@ -128,6 +128,7 @@ template <typename T>
 struct SolverT : public fg_solver {
     DevBuf dNbr, dFlags, dGeo, dVol, dVolP, dNew2Old, dHaloStart, dHaloIds, dSlotLocal;
     DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dBlockMin, dScal, dCnt, dCons, dStage;
+    DevBuf dFIdx, dFGeo, dSlotFace, dClosure, dFB;
     int cur = 0;
     DevMesh<T> dm{};
     PhysT<T> P{};
@@ -136,6 +137,7 @@ struct SolverT : public fg_solver {
 
     Fields<T> fields(int wIn) {
         Fields<T> f;
+        f.FB = dFB.as<T>();
         f.U = dU.as<double>();
         f.U0 = dU0.as<double>();
         f.RHS = dRHS.as<double>();
@@ -256,6 +258,51 @@ struct SolverT : public fg_solver {
             }
             flags[i] = fl;
         }
+        // faces in GPU order: by owner cell (renumbered), then owner slot, so the owners of
+        // consecutive faces are consecutive cells
+        std::vector<int32_t> gFace(nF, -1), slotFace(S, -1), fIdx(2 * (size_t)nF);
+        int nG = 0;
+        for (int i = 0; i < n; i++) {
+            const int o = m.new2old[i];
+            const int nfc = flags[i] & 7;
+            for (int k = 0; k < nfc; k++)
+                if ((flags[i] >> (3 + k)) & 1) gFace[elFc2fc[(size_t)o * 6 + k]] = nG++;
+        }
+        if (nG != nF) return set_err(FG_ERR_MESH, "internal: face ownership does not cover every face");
+        // face geometry: 11 components (n[3], A, x_f - x_owner [3], x_f - x_nb [3], mean volume)
+        const size_t FS = ((size_t)nF * sizeof(T) + 15) / 16 * 16 / sizeof(T);
+        std::vector<T> fgeo(11 * FS, (T)0);
+        for (int f = 0; f < nF; f++) {
+            const int g = gFace[f];
+            const int own = m.fc2el[2 * f], nbo = m.fc2el[2 * f + 1];
+            const int bc = m.boundCond[f];
+            fIdx[g] = m.old2new[own];
+            fIdx[(size_t)nF + g] = (bc == 0) ? m.old2new[nbo] : -bc;
+            for (int d = 0; d < 3; d++) fgeo[(size_t)d * FS + g] = (T)m.n[(size_t)f * 3 + d];
+            fgeo[3 * FS + g] = (T)m.area[f];
+            for (int d = 0; d < 3; d++) {
+                const double xf = m.fcCenter[(size_t)f * 3 + d];
+                fgeo[(size_t)(4 + d) * FS + g] = (T)(xf - m.cellCenter[(size_t)own * 3 + d]);
+                if (bc == 0)
+                    fgeo[(size_t)(7 + d) * FS + g] =
+                        (T)((xf + m.nbShift[(size_t)f * 3 + d]) - m.cellCenter[(size_t)nbo * 3 + d]);
+            }
+            fgeo[10 * FS + g] = (T)((bc == 0) ? (m.volume[own] + m.volume[nbo]) * 0.5 : m.volume[own]);
+        }
+        // slot -> face, and each cell's sum of outward n A (closes to rounding on a closed cell)
+        std::vector<double> clo(3 * (size_t)n, 0.0);
+        for (int i = 0; i < n; i++) {
+            const int o = m.new2old[i];
+            const int nfc = flags[i] & 7;
+            for (int k = 0; k < nfc; k++) {
+                const int f = elFc2fc[(size_t)o * 6 + k];
+                slotFace[(size_t)i * nSlots + k] = gFace[f];
+                const double sg = ((flags[i] >> (3 + k)) & 1) ? 1.0 : -1.0;
+                for (int d = 0; d < 3; d++) clo[(size_t)d * n + i] += sg * m.n[(size_t)f * 3 + d] * m.area[f];
+            }
+        }
+        std::vector<T> closure(3 * (size_t)n);
+        for (size_t q = 0; q < closure.size(); q++) closure[q] = (T)clo[q];
         // shared-memory staging plan: per block of B consecutive cells, the list of face
         // neighbours outside the block and each slot's index among the staged records
         const int B = StageCells<T>::value;
@@ -320,6 +367,16 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(cudaMemcpy(dVol.p, vol.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dVolP.p, volP.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dNew2Old.p, m.new2old.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(dFIdx.alloc(2 * (size_t)nF * sizeof(int32_t)));
+        FG_CUDA_TRY(dFGeo.alloc(11 * FS * sizeof(T)));
+        FG_CUDA_TRY(dSlotFace.alloc(S * sizeof(int32_t)));
+        FG_CUDA_TRY(dClosure.alloc(3 * (size_t)n * sizeof(T)));
+        FG_CUDA_TRY(dFB.alloc((size_t)nF * FREC * sizeof(T)));
+        FG_CUDA_TRY(cudaMemcpy(dFIdx.p, fIdx.data(), 2 * (size_t)nF * sizeof(int32_t), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dFGeo.p, fgeo.data(), 11 * FS * sizeof(T), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dSlotFace.p, slotFace.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dClosure.p, closure.data(), 3 * (size_t)n * sizeof(T), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemset(dFB.p, 0, (size_t)nF * FREC * sizeof(T)));
         const size_t u = (size_t)n * NV * sizeof(double);
         FG_CUDA_TRY(dU.alloc(u));
         FG_CUDA_TRY(dU0.alloc(u));
@@ -329,7 +386,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dW[1].alloc((size_t)n * WREC * sizeof(T)));
         FG_CUDA_TRY(dG.alloc((size_t)n * GREC * sizeof(T)));
         FG_CUDA_TRY(dSig.alloc((size_t)n * sizeof(double)));
-        FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n, StageCells<T>::value), cons_blocks(n)) * sizeof(double)));
+        FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n), cons_blocks(n)) * sizeof(double)));
         FG_CUDA_TRY(dScal.alloc(4 * sizeof(double)));   // dt, time, cons
         FG_CUDA_TRY(dCnt.alloc(4 * sizeof(int32_t)));
         FG_CUDA_TRY(cudaMemset(dU.p, 0, u));
@@ -342,7 +399,8 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(cudaMemcpy(dScal.p, scal, sizeof(scal), cudaMemcpyHostToDevice));
         bytes = 0;
         for (DevBuf *b : {&dNbr, &dFlags, &dGeo, &dVol, &dVolP, &dNew2Old, &dU, &dU0, &dRHS, &dStage, &dW[0], &dW[1], &dG,
-                          &dSig, &dBlockMin, &dScal, &dCnt, &dHaloStart, &dHaloIds, &dSlotLocal})
+                          &dSig, &dBlockMin, &dScal, &dCnt, &dHaloStart, &dHaloIds, &dSlotLocal, &dFIdx, &dFGeo,
+                          &dSlotFace, &dClosure, &dFB})
             bytes += b->bytes;
         dm.n = n;
         dm.nSlots = nSlots;
@@ -355,6 +413,21 @@ struct SolverT : public fg_solver {
         dm.dnx = g + 7 * GS; dm.dny = g + 8 * GS; dm.dnz = g + 9 * GS;
         dm.vol = dVol.as<double>();
         dm.volP = dVolP.as<double>();
+        dm.nF = nF;
+        dm.fStride = FS;
+        dm.fOwn = dFIdx.as<int32_t>();
+        dm.fNb = dFIdx.as<int32_t>() + nF;
+        {
+            const T *fg = dFGeo.as<T>();
+            dm.fnx = fg; dm.fny = fg + FS; dm.fnz = fg + 2 * FS; dm.fA = fg + 3 * FS;
+            for (int d = 0; d < 3; d++) {
+                dm.fdo[d] = fg + (4 + d) * FS;
+                dm.fdn[d] = fg + (7 + d) * FS;
+            }
+            dm.fVavg = fg + 10 * FS;
+        }
+        dm.slotFace = dSlotFace.as<int32_t>();
+        dm.closure = dClosure.as<T>();
         if (stage_kernels_setup<T>(dm) != 0)
             return set_err(FG_ERR_CUDA, "stage kernels need more shared memory than the device allows (halo " +
                                             std::to_string(maxHalo) + " cells)");
@@ -395,14 +468,17 @@ struct SolverT : public fg_solver {
         launch_grad<T>(dm, f, P, s);
         prof_end(s);
         prof_begin(FG_K_FLUX, s);
-        launch_flux<T>(dm, f, P, D, FLUX_RHS, wantSignal, coef(0, 0), s);
+        launch_face<T>(dm, f, P, wantSignal, s);
+        prof_end(s);
+        prof_begin(FG_K_GATHER, s);
+        launch_gather<T>(dm, f, D, FLUX_RHS, wantSignal, coef(0, 0), s);
         prof_end(s);
         FG_LAUNCH_CHECK("compute_rhs");
         return FG_OK;
     }
     int time_step(double *dtOut, cudaStream_t s) override {
         prof_begin(FG_K_DT, s);
-        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(n, StageCells<T>::value), cs.cfl, cs.maxDt, dScal.as<double>(), s);
+        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(n), cs.cfl, cs.maxDt, dScal.as<double>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("time_step");
         if (dtOut) {
@@ -433,7 +509,10 @@ struct SolverT : public fg_solver {
         launch_grad<T>(dm, f, P, s);
         prof_end(s);
         prof_begin(FG_K_FLUX, s);
-        launch_flux<T>(dm, f, P, D, FLUX_FUSED, 0, coef(irk, writeU0), s);
+        launch_face<T>(dm, f, P, 0, s);
+        prof_end(s);
+        prof_begin(FG_K_GATHER, s);
+        launch_gather<T>(dm, f, D, FLUX_FUSED, 0, coef(irk, writeU0), s);
         prof_end(s);
         FG_LAUNCH_CHECK("stage");
         cur ^= 1;

@@ -229,10 +229,11 @@ int fg_step(fg_solver *s, void *stream);
  * (the reference has per-phase cudaEvent timers commented out, e.g. DP/computeRHS.cu:221-235)
  * With profiling enabled every kernel launch of the solver is bracketed by CUDA events on the
  * stream it is launched on; fg_profile_read synchronises and returns per-kind totals.
- * Kinds: 0 gradient+limiter, 1 flux+gather+RK, 2 RK update, 3 relaxation, 4 dt reduction,
- *        5 conservation, 6 other (state copies, time advance). */
+ * Kinds: 0 gradient+limiter, 1 face flux, 2 RK update from the residual buffer, 3 relaxation,
+ *        4 dt reduction, 5 conservation, 6 other (state copies, time advance),
+ *        7 owner-side gather (+ RK combination in a fused stage). */
 enum { FG_K_GRAD = 0, FG_K_FLUX = 1, FG_K_UPDATE = 2, FG_K_RELAX = 3, FG_K_DT = 4, FG_K_CONS = 5, FG_K_OTHER = 6,
-       FG_K_NKINDS = 8 };
+       FG_K_GATHER = 7, FG_K_NKINDS = 8 };
 typedef struct fg_kernel_times {
     double  ms[FG_K_NKINDS];
     int64_t launches[FG_K_NKINDS];
