@@ -87,6 +87,7 @@ SIGNATURES = {
     "fg_stage": (C.c_int, [VP, i32, VP]),
     "fg_relaxation": (C.c_int, [VP, C.POINTER(FgRelaxStats), VP]),
     "fg_cons_calc": (C.c_int, [VP, i32, PD, VP]),
+    "fg_cons_integral_noalloc": (C.c_int, [VP, VP, i32, i32, VP, VP]),
     "fg_get_time": (C.c_int, [VP, PD, PD, PI]),
     "fg_set_dt": (C.c_int, [VP, f64]),
     "fg_step": (C.c_int, [VP, VP]),

@@ -604,6 +604,11 @@ struct SolverT : public fg_solver {
 }  // namespace fg
 
 // ------------------------------------------------------------------ C ABI
+namespace fg {
+// error message setter for the other translation units of the C ABI
+int set_error(int code, const std::string &msg) { return set_err(code, msg); }
+}  // namespace fg
+
 extern "C" {
 
 const char *fg_last_error(void) { return g_err.c_str(); }

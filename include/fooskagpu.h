@@ -217,6 +217,22 @@ int fg_relaxation(fg_solver *s, fg_relax_stats *stats, void *stream);
  * (ivar 0 integrates 1-alpha).  Deterministic two-level reduction. */
 int fg_cons_calc(fg_solver *s, int32_t ivar, double *out, void *stream);
 
+/* Conservation integral without device allocation.  No counterpart in the reference: it is
+ * for callers that cannot call cudaMalloc when they need the integral (an application whose
+ * pool allocator owns all device memory, a monitor between the steps of a latency-critical
+ * loop where cudaMalloc / cudaFree may synchronise the device).
+ * U: device, reference layout U[cell*10 + v]; vol: device, nCells volumes; out: device, one
+ * double, receives the integral of variable ivar (ivar 0 integrates 1-alpha), as fg_cons_calc.
+ * Runs on the calling thread's current device, asynchronously on `stream`.
+ * The block partial sums go to a static device array of FG_NOALLOC_MAX_CELLS/256 doubles
+ * (512 KiB, held on every device that loads the library until exit); nCells above
+ * FG_NOALLOC_MAX_CELLS is rejected with FG_ERR_ARG.  The first call on a device looks the
+ * array's address up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU race. */
+#define FG_NOALLOC_MAX_CELLS (65536 * 256)
+int fg_cons_integral_noalloc(const double *U, const double *vol, int32_t nCells, int32_t ivar, double *out,
+                             void *stream);
+
 /* dt and physical time held by the solver. */
 int fg_get_time(fg_solver *s, double *dt, double *physicalTime, int32_t *iStep);
 int fg_set_dt(fg_solver *s, double dt);
