@@ -293,6 +293,47 @@ def cpu_baseline(mesh, case, U, max_stages=3):
             "sample": f"{stages} RK3 stages (residual + update, FP64) on the full {mesh.n_elem}-cell mesh"}
 
 
+def reference_gpu(args):
+    """The reference's own double-precision CUDA build (oracle/_ref/fooska_ref_dp, compiled from
+    the reference sources by oracle/build_ref.py) on the nearest workload it can express: the
+    same 128^3 hex cube, TGV state and case, with slip walls in place of the periodic faces
+    (the reference has no periodic boundary), elements in the same shuffled order (the reference
+    does not renumber).  Timed by the driver's CUDA events around the step loop."""
+    from oracle import ref_run
+    if not ref_run.available():
+        return {"unavailable": "reference GPU build oracle/_ref/fooska_ref_dp not present (built from the reference sources)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU visible"}
+    except Exception as e:  # pragma: no cover
+        return {"unavailable": f"torch: {e}"}
+    from fooskagpu_b200 import cases, meshgen
+    from fooskagpu_b200.api import Mesh
+    L = 2 * math.pi
+    MESH_DIR.mkdir(parents=True, exist_ok=True)
+    path = MESH_DIR / f"tgv{NCELL_SIDE}_slip_shuffled.neu"
+    if not path.exists():
+        meshgen.write_neu(str(path), meshgen.box_hexes(NCELL_SIDE, NCELL_SIDE, NCELL_SIDE, L=(L, L, L), shuffle=True,
+                                                       seed=20261203))
+    mesh = Mesh.load_neu(str(path), scale=1.0)
+    case = cases.tgv_case()
+    U = cases.tgv_ic(case, mesh.arrays()["cellCenter"])
+    nE = mesh.n_elem
+    mesh.close()
+    steps, warm = max(1, min(args.steps, 20)), 3
+    try:
+        rep = ref_run.run(MESH_DIR / "ref_workdir", path, case, U, steps, warm, timeout=600)
+    except Exception as e:
+        return {"unavailable": f"reference GPU run failed: {str(e)[:300]}"}
+    ms = rep["ms"]
+    return {"value": nE * case.rkSteps * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "warmup": warm, "cells": nE, "status": rep["status"], "dtype": "f64",
+            "workload": f"tgv_les_wale_{NCELL_SIDE}^3_hex, slip walls (no periodic BC in the reference), "
+                        "shuffled element order (no renumbering in the reference)",
+            "build": "reference DP sources, nvcc 12.9 -gencode sm_100a -rdc, -maxrregcount=128, single-rank MPI/METIS stubs"}
+
+
 def run_reference(args):
     """Reference arm: the reference's path has no CPU implementation of its own, so this times
     the FP64 CPU restatement of it (oracle) with all host threads on the same workload."""
@@ -307,8 +348,14 @@ def run_reference(args):
     O.set_threads(th)
     o = O.Oracle(mesh.view(), case)
     Uc = U.copy()
-    for _ in range(min(args.warmup, 1)):
+    tw = time.perf_counter()
+    o.init_rk(Uc)
+    for w in range(args.warmup):   # warm-up stages on a copy of the state
         o.residual(Uc)
+        o.update(w % 3, 1e-4, Uc)
+        if time.perf_counter() - tw > 60:
+            break
+    Uc = U.copy()
     steps = 0
     cap = max(1, min(args.steps, args.cpu_stages))
     t0 = time.perf_counter()
@@ -323,13 +370,14 @@ def run_reference(args):
     val = mesh.n_elem * steps / dt
     sample = f"{steps} RK3 stages (one stage per step) on the full {mesh.n_elem}-cell mesh"
     return dict(
-        impl="reference", metric=METRIC, value=val, unit=UNIT, n_gpus=1, steps=steps, warmup=min(args.warmup, 1),
+        impl="reference", metric=METRIC, value=val, unit=UNIT, n_gpus=1, steps=steps, warmup=args.warmup,
         ms_per_step=dt * 1e3 / steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
         data="synthetic",
         config={"workload": f"tgv_les_wale_{NCELL_SIDE}^3_hex_periodic", "cells": mesh.n_elem, "rk_stages": 3},
         cpu_baseline={"kind": "port", "cores": th, "sample": sample, "value": val, "unit": UNIT},
         e2e={"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         note="the reference implements this path only in CUDA; its CPU arm is the FP64 C++ restatement (oracle)",
+        reference_gpu=reference_gpu(args) if not args.no_ref_gpu else None,
     )
 
 
@@ -341,6 +389,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-stages", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="reference arm: skip timing the reference GPU build")
     ap.add_argument("--n", type=int, default=None, help="cells per side of the TGV cube (default 128)")
     args = ap.parse_args()
     if args.n:

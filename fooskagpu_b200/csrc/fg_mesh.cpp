@@ -375,9 +375,9 @@ int finish_mesh(Mesh &m, const fg_mesh_opts &o, std::string &err) {
         double span = 0;
         for (int d = 0; d < 3; d++) span = std::max(span, hi[d] - lo[d]);
         const double tol = 1e-7 * (span > 0 ? span : 1.0);
-        // key: face centre wrapped into the periodic box, quantised by tol
-        auto keyOf = [&](const double *c) {
-            std::array<int64_t, 3> k;
+        // face centre wrapped into the periodic box; faces whose wrapped centres are within tol
+        // (per axis, modulo L) are periodic images of each other
+        auto wrap = [&](const double *c, double *w) {
             for (int d = 0; d < 3; d++) {
                 double v = c[d];
                 if (L[d] > 0) {
@@ -385,8 +385,13 @@ int finish_mesh(Mesh &m, const fg_mesh_opts &o, std::string &err) {
                     v = v - L[d] * std::floor(v / L[d] + 0.5 * tol / L[d]);
                     if (v > L[d] - tol) v -= L[d];
                 }
-                k[d] = (int64_t)std::llround(v / (4 * tol));
+                w[d] = v;
             }
+        };
+        // hash grid of cell size 4 tol: an image lies in the same or an adjacent cell
+        auto cellOf = [&](const double *w) {
+            std::array<int64_t, 3> k;
+            for (int d = 0; d < 3; d++) k[d] = (int64_t)std::floor(w[d] / (4 * tol));
             return k;
         };
         struct AH {
@@ -394,35 +399,56 @@ int finish_mesh(Mesh &m, const fg_mesh_opts &o, std::string &err) {
                 return (size_t)(a[0] * 73856093LL ^ a[1] * 19349663LL ^ a[2] * 83492791LL);
             }
         };
-        std::unordered_map<std::array<int64_t, 3>, int64_t, AH> pmap;
-        pmap.reserve(unmatched.size());
-        std::vector<int64_t> still;
-        for (int64_t ef : unmatched) {
-            const double *c = &m.elFcCenter[(size_t)ef * 3];
-            auto k = keyOf(c);
-            auto it = pmap.find(k);
-            if (it == pmap.end()) {
-                pmap.emplace(k, ef);
-            } else {
-                const int64_t other = it->second;
-                const int e = (int)(ef / 6), f = (int)(ef % 6), e1 = (int)(other / 6), f1 = (int)(other % 6);
-                m.neig[(size_t)e * 6 + f] = e1;
-                m.neigFc[(size_t)e * 6 + f] = f1;
-                m.neig[(size_t)e1 * 6 + f1] = e;
-                m.neigFc[(size_t)e1 * 6 + f1] = f;
-                for (int d = 0; d < 3; d++) {
-                    // position of the shared face as seen from the other element
-                    const double sh = m.elFcCenter[(size_t)other * 3 + d] - m.elFcCenter[(size_t)ef * 3 + d];
-                    const double q = (L[d] > 0) ? L[d] * std::llround(sh / L[d]) : 0.0;
-                    m.neigShift[(size_t)e * 18 + f * 3 + d] = q;    // face of e seen from e1 = centre(e) + q
-                    m.neigShift[(size_t)e1 * 18 + f1 * 3 + d] = -q;
-                }
-                m.nPeriodic++;
-                pmap.erase(it);
-            }
+        const size_t nU = unmatched.size();
+        std::vector<double> wc(nU * 3);
+        std::unordered_map<std::array<int64_t, 3>, std::vector<int64_t>, AH> grid;
+        grid.reserve(nU);
+        for (size_t i = 0; i < nU; i++) {
+            wrap(&m.elFcCenter[(size_t)unmatched[i] * 3], &wc[i * 3]);
+            grid[cellOf(&wc[i * 3])].push_back((int64_t)i);
         }
-        unmatched.clear();
-        for (auto &kv : pmap) unmatched.push_back(kv.second);
+        std::vector<char> done(nU, 0);
+        auto near = [&](size_t i, size_t j) {
+            for (int d = 0; d < 3; d++) {
+                double dd = std::fabs(wc[i * 3 + d] - wc[j * 3 + d]);
+                if (L[d] > 0) dd = std::min(dd, std::fabs(L[d] - dd));
+                if (dd > tol) return false;
+            }
+            return true;
+        };
+        for (size_t i = 0; i < nU; i++) {
+            if (done[i]) continue;
+            const auto k0 = cellOf(&wc[i * 3]);
+            int64_t best = -1;
+            for (int a = -1; a <= 1; a++)
+                for (int b = -1; b <= 1; b++)
+                    for (int c = -1; c <= 1; c++) {
+                        auto it = grid.find({k0[0] + a, k0[1] + b, k0[2] + c});
+                        if (it == grid.end()) continue;
+                        for (int64_t j : it->second)
+                            if ((size_t)j != i && !done[j] && near(i, (size_t)j) && (best < 0 || j < best)) best = j;
+                    }
+            if (best < 0) continue;
+            done[i] = done[best] = 1;
+            const int64_t ef = unmatched[i], other = unmatched[best];
+            const int e = (int)(ef / 6), f = (int)(ef % 6), e1 = (int)(other / 6), f1 = (int)(other % 6);
+            m.neig[(size_t)e * 6 + f] = e1;
+            m.neigFc[(size_t)e * 6 + f] = f1;
+            m.neig[(size_t)e1 * 6 + f1] = e;
+            m.neigFc[(size_t)e1 * 6 + f1] = f;
+            for (int d = 0; d < 3; d++) {
+                // position of the shared face as seen from the other element
+                const double sh = m.elFcCenter[(size_t)other * 3 + d] - m.elFcCenter[(size_t)ef * 3 + d];
+                const double q = (L[d] > 0) ? L[d] * std::llround(sh / L[d]) : 0.0;
+                m.neigShift[(size_t)e * 18 + f * 3 + d] = q;    // face of e seen from e1 = centre(e) + q
+                m.neigShift[(size_t)e1 * 18 + f1 * 3 + d] = -q;
+            }
+            m.nPeriodic++;
+        }
+        std::vector<int64_t> still;
+        for (size_t i = 0; i < nU; i++)
+            if (!done[i]) still.push_back(unmatched[i]);
+        unmatched.swap(still);
     }
     if (!unmatched.empty()) {
         const int64_t ef = *std::min_element(unmatched.begin(), unmatched.end());

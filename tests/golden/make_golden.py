@@ -19,7 +19,6 @@ from __future__ import annotations
 import ctypes as C
 import json
 import os
-import subprocess
 import sys
 from pathlib import Path
 
@@ -206,19 +205,6 @@ def ic_for(spec, c, centres):
     return cases.sod_ic(c, centres, x0=0.0)
 
 
-def write_case_file(path, c):
-    with open(path, "w") as f:
-        for k, t in type(c)._fields_:
-            if k in ("relaxFlag", "hllcEnergyFix", "hllcTieTol", "reserved"):
-                continue
-            v = getattr(c, k)
-            if hasattr(v, "__len__"):
-                for i in range(len(v)):
-                    f.write(f"{k}[{i}] = {v[i]!r}\n")
-            else:
-                f.write(f"{k} = {v!r}\n")
-
-
 def centres_of(mesh: meshgen.NeuMesh):
     cs = []
     for blk in mesh.elems:
@@ -227,7 +213,7 @@ def centres_of(mesh: meshgen.NeuMesh):
 
 
 def run_stage_fixtures(outdir):
-    exe = ROOT / "oracle" / "_ref" / "fooska_ref_dp"
+    from oracle import ref_run
     outdir = Path(outdir).resolve()
     for spec in stage_specs():
         wd = outdir / spec["name"]
@@ -235,12 +221,11 @@ def run_stage_fixtures(outdir):
         m, c = build_spec(spec)
         meshgen.write_neu(str(wd / "sh.neu"), m)
         U = ic_for(spec, c, centres_of(m))
-        U.astype(np.float64).tofile(wd / "ic.bin")
-        write_case_file(wd / "case.txt", c)
-        r = subprocess.run([str(exe), str(wd), str(wd / "case.txt"), str(wd / "ic.bin"), str(spec["steps"]), "--dump"],
-                           capture_output=True, text=True, timeout=300)
-        (wd / "log.txt").write_text(r.stdout[-20000:] + r.stderr[-20000:])
-        print(spec["name"], r.returncode, r.stdout.strip().splitlines()[-1:] if r.stdout else "")
+        try:
+            rep = ref_run.run(wd, wd / "sh.neu", c, U, spec["steps"], dump=True)
+            print(spec["name"], rep)
+        except Exception as e:  # keep going: one failing case should not hide the others
+            print(spec["name"], "failed:", e)
 
 
 def collect_stage_fixtures(outdir):
