@@ -63,7 +63,7 @@ KERNEL_KINDS = ["grad", "flux", "update", "relax", "dt", "cons", "other", "gathe
 
 
 class FgRelaxStats(C.Structure):
-    _fields_ = [("nTherm", i32), ("nChem", i32), ("nAbort", i32), ("reserved", i32)]
+    _fields_ = [("nTherm", i32), ("nChem", i32), ("nAbort", i32), ("nIter", i32)]
 
 
 # name -> (restype, argtypes); every symbol here is declared in include/fooskagpu.h

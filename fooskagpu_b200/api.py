@@ -138,7 +138,7 @@ class Solver:
     def relaxation(self, stream=None) -> dict:
         st = FgRelaxStats()
         check(lib().fg_relaxation(self._h, C.byref(st), stream))
-        return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort}
+        return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter}
 
     def cons_calc(self, ivar: int, stream=None) -> float:
         v = C.c_double()

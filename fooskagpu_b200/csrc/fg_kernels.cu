@@ -201,7 +201,7 @@ __device__ __forceinline__ void stage_geometry(const DevMesh<T> &m, int lo, int 
 
 // ------------------------------------------------------------------ gradient + limiter
 template <typename T>
-__global__ void __launch_bounds__(StageCells<T>::value) k_grad(const DevMesh<T> m, const T *__restrict__ W,
+__global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_grad(const DevMesh<T> m, const T *__restrict__ W,
                                                                 T *__restrict__ G, const PhysT<T> P) {
     constexpr int WS = Stage<T>::WS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -318,7 +318,7 @@ __device__ __forceinline__ void face_state(const T *w, const T *g, T dx, T dy, T
 //   var 0: -alpha_c s u,  vars 6/7: +alpha_c pL_c s u, +(1-alpha_c) pG_c s u,
 //   momentum: -pC_c s A n summed = pC_c * (sum of outward n A)  (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
 template <typename T>
-__global__ void __launch_bounds__(128) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
+__global__ void __launch_bounds__(128, MinBlocks<T>::face) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
                                               T *__restrict__ FB, const PhysT<T> P, int wantSignal) {
     const int fi = blockIdx.x * blockDim.x + threadIdx.x;
     if (fi >= m.nF) return;
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(128) k_face(const DevMesh<T> m, const T *__res
 
 // ------------------------------------------------------------------ owner-side gather + RK
 template <typename T>
-__global__ void __launch_bounds__(256) k_gather(const DevMesh<T> m, Fields<T> f, const PhysD D, int mode,
+__global__ void __launch_bounds__(256, MinBlocks<T>::gather) k_gather(const DevMesh<T> m, Fields<T> f, const PhysD D, int mode,
                                                 int wantSignal, StageCoef sc) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;

@@ -55,7 +55,7 @@ __device__ __forceinline__ void therm_res(const Ph *h, int pm, double *x, const 
     *r1 = t_of(h[0], x[0], x[2]) - t_of(h[1], x[1], x[3]);
 }
 
-__device__ int therm_cell(const RelaxParams &R, const Ph *h, double *U) {
+__device__ int therm_cell(const RelaxParams &R, const Ph *h, double *U, int *iters) {
     double ar[2], enr[2], x[4], ax[4];
     const double a0 = fmin(fmax(R.avfMin / 100, U[0]), 1 - R.avfMin / 100);
     const double a1 = 1 - a0;
@@ -77,6 +77,7 @@ __device__ int therm_cell(const RelaxParams &R, const Ph *h, double *U) {
     float minRes = 1e9f;
     int abortFlag = 0, aborted = 0;
     for (int itr = 1;; itr++) {
+        *iters = itr;
         double res[2], rdf[2][2], e[2];
         therm_res(h, pm, x, ar, enr, &res[0], &res[1]);
         // finite-difference Jacobian over the minor phase's (rho, e)
@@ -168,7 +169,7 @@ __device__ void chem_check(const RelaxParams &R, double xOld, double *x, double 
     }
 }
 
-__device__ int chem_cell(const RelaxParams &R, const Ph *h, double *U) {
+__device__ int chem_cell(const RelaxParams &R, const Ph *h, double *U, int *iters) {
     double x[6], ax[6];
     x[0] = fmin(fmax(R.avfMin / 100, U[0]), 1 - R.avfMin / 100);
     x[1] = 1 - x[0];
@@ -186,6 +187,7 @@ __device__ int chem_cell(const RelaxParams &R, const Ph *h, double *U) {
     float minRes = 1e9f;
     int abortFlag = 0, aborted = 0;
     for (int itr = 1;; itr++) {
+        *iters = itr;
         double res[3], rdf[3][3], e[3];
         chem_res(R, h, pm, x, rm, re, res);
         const int js[3] = {mm, mm + 2, mm + 4};
@@ -265,7 +267,7 @@ __device__ int chem_cell(const RelaxParams &R, const Ph *h, double *U) {
 template <typename T>
 __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R, int32_t *counters) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    int chem = 0, ab = 0;
+    int chem = 0, ab = 0, its = 0;
     const bool act = c < n;
     if (act) {
         double u[NV];
@@ -281,7 +283,7 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
             const double ts = sat_temp(R, pl, tl, R.satTempUrf);
             chem = (tl > ts && avf > R.chemLimit);
         }
-        ab = chem ? chem_cell(R, h, u) : therm_cell(R, h, u);
+        ab = chem ? chem_cell(R, h, u, &its) : therm_cell(R, h, u, &its);
         U[(size_t)0 * n + c] = u[0];
         U[(size_t)1 * n + c] = u[1];
         U[(size_t)2 * n + c] = u[2];
@@ -296,14 +298,16 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
 #pragma unroll
         for (int v = NP; v < WREC; v++) p[v] = 0;
     }
-    // warp-aggregated counters (counts only: order does not matter)
+    // warp-aggregated counters (sums of integers: order does not matter)
     const unsigned mask = __ballot_sync(0xffffffffu, act && chem);
     const unsigned maskT = __ballot_sync(0xffffffffu, act && !chem);
     const unsigned maskA = __ballot_sync(0xffffffffu, act && ab);
+    const int itsW = __reduce_add_sync(0xffffffffu, its);
     if ((threadIdx.x & 31) == 0) {
         if (maskT) atomicAdd(&counters[0], __popc(maskT));
         if (mask) atomicAdd(&counters[1], __popc(mask));
         if (maskA) atomicAdd(&counters[2], __popc(maskA));
+        if (itsW) atomicAdd(&counters[3], itsW);
     }
 }
 

@@ -531,7 +531,7 @@ struct SolverT : public fg_solver {
             st->nTherm = h[0];
             st->nChem = h[1];
             st->nAbort = h[2];
-            st->reserved = 0;
+            st->nIter = h[3];
         }
         return FG_OK;
     }

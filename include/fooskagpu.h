@@ -209,7 +209,7 @@ typedef struct fg_relax_stats {
     int32_t nTherm;       /* cells relaxed thermally          */
     int32_t nChem;        /* cells relaxed chemically         */
     int32_t nAbort;       /* Newton solves that fell back to the best iterate */
-    int32_t reserved;
+    int32_t nIter;        /* Newton iterations summed over all cells */
 } fg_relax_stats;
 int fg_relaxation(fg_solver *s, fg_relax_stats *stats, void *stream);
 

@@ -1038,8 +1038,8 @@ void orc_update(const fg_case *c, const fg_mesh_view *m, int irk, double dt, dou
 /* relaxation (DP/relaxation.cu:46-114) */
 void orc_relaxation(const fg_case *c, const fg_mesh_view *m, double *U, fg_relax_stats *st) {
     const int nE = m->nElem;
-    int nT = 0, nC = 0, nA = 0;
-#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 256) reduction(+ : nT, nC, nA)
+    int nT = 0, nC = 0, nA = 0, nI = 0;
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 256) reduction(+ : nT, nC, nA, nI)
     for (int cI = 0; cI < nE; cI++) {
         double *u = U + (size_t)cI * 10;
         int chem = 0;
@@ -1057,8 +1057,9 @@ void orc_relaxation(const fg_case *c, const fg_mesh_view *m, double *U, fg_relax
         int it = 0;
         if (chem) { nA += chem_relax_cell(c, u, &it); nC++; }
         else { nA += therm_relax_cell(c, u, &it); nT++; }
+        nI += it;
     }
-    if (st) { st->nTherm = nT; st->nChem = nC; st->nAbort = nA; st->reserved = 0; }
+    if (st) { st->nTherm = nT; st->nChem = nC; st->nAbort = nA; st->nIter = nI; }
 }
 
 /* integrateConsVar + consCalc (DP/consCalc.cu:3-60); fixed 4096-cell chunks so the result

@@ -128,7 +128,7 @@ class Oracle:
         from fooskagpu_b200._lib import FgRelaxStats
         st = FgRelaxStats()
         lib().orc_relaxation(C.byref(self.case), C.byref(self.view), _p(U), C.byref(st))
-        return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort}
+        return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter}
 
     def cons_calc(self, ivar: int, U: np.ndarray) -> float:
         return lib().orc_cons_calc(C.byref(self.view), ivar, _p(np.ascontiguousarray(U)))

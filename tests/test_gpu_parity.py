@@ -146,6 +146,8 @@ def test_relaxation(name, meshdir):
     e = rel_err(Ug, Uo)
     _report(f"relax/{name}", dict(state=e.tolist(), oracle=st_o, gpu=st_g))
     assert st_g["nChem"] == st_o["nChem"] and st_g["nTherm"] == st_o["nTherm"]
+    # the same Newton iteration counts and aborts cell for cell, summed
+    assert st_g["nIter"] == st_o["nIter"] and st_g["nAbort"] == st_o["nAbort"], (st_g, st_o)
     assert st_o["nChem"] > 0, "fixture should exercise the chemical branch"
     assert e.max() < TOL["fp64"]["relax"], e
     s.close()
