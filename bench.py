@@ -264,10 +264,94 @@ def run_ours(args, rank, world, local_rank, dist):
         kernels_fp64={k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]} for k, v in prof64.items()},
         clocks=cl,
     )
+    # ---------------- two-phase workload with the Gibbs relaxation and the learned surrogate
+    if not args.no_two_phase:
+        out["two_phase"] = two_phase(args, torch, stream, dev)
     # ---------------- CPU baseline (rank 0, N = 1 only): oracle FP64 on the host cores
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, case, U0, max_stages=args.cpu_stages)
     return out
+
+
+def two_phase(args, torch, stream, dev):
+    """Two-phase workload with the chemical (Gibbs) relaxation active: the reference's own fluid
+    constants (DP/buildInput.cu) on a cube of NTP^3 hexes with slip walls and a smoothly
+    perturbed liquid/vapour state (about half of the cells need the Gibbs solve each step).
+    FP64 Newton-only vs mixed precision with and without the learned surrogate; the surrogate is
+    trained inside this run on samples logged from the FP64 run's first steps."""
+    from fooskagpu_b200 import cases, meshgen
+    from fooskagpu_b200.api import Mesh, Solver, Surrogate
+    ntp = int(os.environ.get("FG_BENCH_TP_N", "96"))
+    MESH_DIR.mkdir(parents=True, exist_ok=True)
+    path = MESH_DIR / f"two_phase_box{ntp}.neu"
+    if not path.exists():
+        meshgen.write_neu(str(path), meshgen.box_hexes(ntp, ntp, ntp, L=(0.02, 0.02, 0.02)))
+    mesh = Mesh.load_neu(str(path), scale=1.0)
+    case = cases.reference_case()
+    case.rkSteps = 3
+    case.hllcTieTol = 1e-4
+    U0 = cases.perturbed_two_phase_ic(case, mesh.arrays()["cellCenter"], seed=5, vel=25.0)
+    nE = mesh.n_elem
+    steps, warm = max(5, min(args.steps, 20)), 3
+    res = {"workload": f"two_phase_reference_fluid_{ntp}^3_hex_slip", "cells": nE, "steps": steps, "warmup": warm}
+
+    def run(prec, sg=None, log=0):
+        s = Solver(mesh, case, precision=prec, device=dev)
+        s.set_state(U0)
+        if log:
+            s.relax_log(log)
+        if sg is not None:
+            s.set_surrogate(sg, 1e-6, 3)
+        for _ in range(warm):
+            s.step(stream=stream.cuda_stream)
+        data = s.relax_log_read(log) if log else None
+        if log:
+            s.relax_log(0)
+        ms = time_steps(s, steps, torch, stream)
+        st = s.relax_stats()                           # the last timed step's relaxation
+        U = s.get_state()
+        s.profile(True)
+        time_steps(s, 2, torch, stream)
+        prof = s.profile_read()
+        s.profile(False)
+        s.close()
+        return ms, prof, st, U, data
+
+    ms64, p64, st64, U64, (X, Y) = run("fp64", log=4_000_000)
+    res["fp64_value"] = nE * 3 * steps / (ms64 / 1e3)
+    res["fp64_relax_ms"] = p64["relax"]["ms"] / p64["relax"]["launches"]
+    g = Surrogate(device=dev, seed=1)
+    t0 = time.perf_counter()
+    take = min(len(X), 1_000_000)
+    g.set_data(X[:take], Y[:take])
+    loss = g.train(15, batch=2048, lr=2e-3, seed=2)
+    res["surrogate_training"] = {"samples": take, "epochs": 15, "final_loss": loss,
+                                 "seconds": time.perf_counter() - t0}
+    msm, pm, stm, Um, _ = run("mixed")
+    mss, ps, sts, Us, _ = run("mixed", sg=g)
+    res["mixed_value"] = nE * 3 * steps / (msm / 1e3)
+    res["mixed_relax_ms"] = pm["relax"]["ms"] / pm["relax"]["launches"]
+    res["value"] = nE * 3 * steps / (mss / 1e3)
+    res["relax_ms"] = ps["relax"]["ms"] / ps["relax"]["launches"]
+    res["mixed_surrogate_over_fp64"] = res["value"] / res["fp64_value"]
+    res["chem_cells"] = sts["nChem"]
+    res["fallback_rate"] = sts["nFallback"] / max(1, sts["nChem"])
+    res["newton_iters_per_cell"] = {"fp64_newton": st64["nIter"] / max(1, st64["nChem"] + st64["nTherm"]),
+                                    "mixed_newton": stm["nIter"] / max(1, stm["nChem"] + stm["nTherm"]),
+                                    "mixed_surrogate": sts["nIter"] / max(1, sts["nChem"] + sts["nTherm"])}
+    rho = lambda U: U[:, 1] + U[:, 2]
+    res["rho_rel_l2_vs_fp64"] = float(np.linalg.norm(rho(Us) - rho(U64)) / np.linalg.norm(rho(U64)))
+
+    def p_liq(U):
+        al = np.clip(U[:, 0], case.avfMin / 100, 1 - case.avfMin / 100)
+        r = U[:, 1] / al
+        gm = case.gamma[0]
+        return (gm - 1) * r * (U[:, 6] / U[:, 1]) - gm * case.pInf[0] - (gm - 1) * case.eta[0] * r
+
+    res["p_rel_l2_vs_fp64"] = float(np.linalg.norm(p_liq(Us) - p_liq(U64)) / np.linalg.norm(p_liq(U64)))
+    g.close()
+    mesh.close()
+    return res
 
 
 def cpu_baseline(mesh, case, U, max_stages=3):
@@ -390,6 +474,7 @@ def main():
     ap.add_argument("--cpu-stages", type=int, default=6)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="reference arm: skip timing the reference GPU build")
+    ap.add_argument("--no-two-phase", action="store_true", help="skip the two-phase (surrogate) workload")
     ap.add_argument("--n", type=int, default=None, help="cells per side of the TGV cube (default 128)")
     args = ap.parse_args()
     if args.n:

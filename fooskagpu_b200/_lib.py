@@ -15,6 +15,11 @@ f64 = C.c_double
 PD = C.POINTER(C.c_double)
 PI = C.POINTER(C.c_int32)
 VP = C.c_void_p
+PF = C.POINTER(C.c_float)
+i64 = C.c_int64
+u64 = C.c_uint64
+SG_NPARAM = 8836
+SG_NNORM = 30
 
 FG_OK, FG_ERR_ARG, FG_ERR_IO, FG_ERR_MESH, FG_ERR_CUDA, FG_ERR_NAN, FG_ERR_UNSUPPORTED, FG_ERR_NOMEM = range(8)
 FG_PREC_FP64, FG_PREC_MIXED = 0, 1
@@ -63,7 +68,8 @@ KERNEL_KINDS = ["grad", "flux", "update", "relax", "dt", "cons", "other", "gathe
 
 
 class FgRelaxStats(C.Structure):
-    _fields_ = [("nTherm", i32), ("nChem", i32), ("nAbort", i32), ("nIter", i32)]
+    _fields_ = [("nTherm", i32), ("nChem", i32), ("nAbort", i32), ("nIter", i32), ("nSurrogate", i32),
+                ("nFallback", i32)]
 
 
 # name -> (restype, argtypes); every symbol here is declared in include/fooskagpu.h
@@ -88,6 +94,20 @@ SIGNATURES = {
     "fg_relaxation": (C.c_int, [VP, C.POINTER(FgRelaxStats), VP]),
     "fg_cons_calc": (C.c_int, [VP, i32, PD, VP]),
     "fg_cons_integral_noalloc": (C.c_int, [VP, VP, i32, i32, VP, VP]),
+    "fg_surrogate_create": (C.c_int, [i32, u64, C.POINTER(VP)]),
+    "fg_surrogate_destroy": (C.c_int, [VP]),
+    "fg_surrogate_set_data": (C.c_int, [VP, PF, PF, i64]),
+    "fg_surrogate_train": (C.c_int, [VP, i32, i32, C.c_float, u64, PF]),
+    "fg_surrogate_loss_grad": (C.c_int, [VP, PF, PF, i32, PF, PF]),
+    "fg_surrogate_get_params": (C.c_int, [VP, PF]),
+    "fg_surrogate_set_params": (C.c_int, [VP, PF]),
+    "fg_surrogate_get_norm": (C.c_int, [VP, PF]),
+    "fg_surrogate_set_norm": (C.c_int, [VP, PF]),
+    "fg_surrogate_predict": (C.c_int, [VP, PF, i32, PF, PI]),
+    "fg_solver_set_surrogate": (C.c_int, [VP, VP, f64, i32]),
+    "fg_relax_log": (C.c_int, [VP, i64]),
+    "fg_relax_stats_read": (C.c_int, [VP, C.POINTER(FgRelaxStats)]),
+    "fg_relax_log_read": (C.c_int, [VP, PF, PF, i64, C.POINTER(i64)]),
     "fg_get_time": (C.c_int, [VP, PD, PD, PI]),
     "fg_set_dt": (C.c_int, [VP, f64]),
     "fg_step": (C.c_int, [VP, VP]),

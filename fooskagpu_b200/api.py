@@ -138,7 +138,32 @@ class Solver:
     def relaxation(self, stream=None) -> dict:
         st = FgRelaxStats()
         check(lib().fg_relaxation(self._h, C.byref(st), stream))
-        return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter}
+        return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter,
+                "nSurrogate": st.nSurrogate, "nFallback": st.nFallback}
+
+    def relax_stats(self) -> dict:
+        """Counts of the most recent relaxation (also the one inside step())."""
+        st = FgRelaxStats()
+        check(lib().fg_relax_stats_read(self._h, C.byref(st)))
+        return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter,
+                "nSurrogate": st.nSurrogate, "nFallback": st.nFallback}
+
+    # -- learned equilibrium surrogate
+    def set_surrogate(self, sg: Optional["Surrogate"], rel_tol: float = 1e-6, polish_iters: int = 3) -> None:
+        """Attach (or detach with None) the surrogate used by relaxation()/step()."""
+        self._sg = sg
+        check(lib().fg_solver_set_surrogate(self._h, sg._h if sg is not None else None, rel_tol, polish_iters))
+
+    def relax_log(self, capacity: int) -> None:
+        """Log chemical Newton solves as surrogate training samples (0 turns the log off)."""
+        check(lib().fg_relax_log(self._h, int(capacity)))
+
+    def relax_log_read(self, cap: int):
+        X = np.empty((max(cap, 1), 3), dtype=np.float32)
+        Y = np.empty((max(cap, 1), 4), dtype=np.float32)
+        k = C.c_int64()
+        check(lib().fg_relax_log_read(self._h, _fptr(X), _fptr(Y), int(cap), C.byref(k)))
+        return X[:k.value].copy(), Y[:k.value].copy()
 
     def cons_calc(self, ivar: int, stream=None) -> float:
         v = C.c_double()
@@ -196,6 +221,78 @@ class Solver:
     def close(self):
         if getattr(self, "_h", None):
             lib().fg_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Surrogate:
+    """Learned equilibrium surrogate (MLP 3 -> 64 -> 64 -> 64 -> 4): (rho, e, Y) -> (p, T, alpha, Y_eq)."""
+
+    NPARAM = L.SG_NPARAM
+    NNORM = L.SG_NNORM
+
+    def __init__(self, device: int = 0, seed: int = 20261203):
+        h = C.c_void_p()
+        check(lib().fg_surrogate_create(device, seed, C.byref(h)))
+        self._h = h
+
+    def set_data(self, X: np.ndarray, Y: np.ndarray) -> None:
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, 3)
+        Y = np.ascontiguousarray(Y, dtype=np.float32).reshape(-1, 4)
+        check(lib().fg_surrogate_set_data(self._h, _fptr(X), _fptr(Y), len(X)))
+
+    def train(self, epochs: int, batch: int = 4096, lr: float = 2e-3, seed: int = 1) -> float:
+        loss = C.c_float()
+        check(lib().fg_surrogate_train(self._h, epochs, batch, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def loss_grad(self, Xs: np.ndarray, Ys: np.ndarray):
+        """Loss and gradient on standardised samples (no parameter update)."""
+        Xs = np.ascontiguousarray(Xs, dtype=np.float32).reshape(-1, 3)
+        Ys = np.ascontiguousarray(Ys, dtype=np.float32).reshape(-1, 4)
+        g = np.empty(self.NPARAM, dtype=np.float32)
+        loss = C.c_float()
+        check(lib().fg_surrogate_loss_grad(self._h, _fptr(Xs), _fptr(Ys), len(Xs), C.byref(loss), _fptr(g)))
+        return loss.value, g
+
+    def params(self) -> np.ndarray:
+        p = np.empty(self.NPARAM, dtype=np.float32)
+        check(lib().fg_surrogate_get_params(self._h, _fptr(p)))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().fg_surrogate_set_params(self._h, _fptr(p)))
+
+    def norm(self) -> np.ndarray:
+        v = np.empty(self.NNORM, dtype=np.float32)
+        check(lib().fg_surrogate_get_norm(self._h, _fptr(v)))
+        return v
+
+    def set_norm(self, v: np.ndarray) -> None:
+        v = np.ascontiguousarray(v, dtype=np.float32)
+        check(lib().fg_surrogate_set_norm(self._h, _fptr(v)))
+
+    def predict(self, X: np.ndarray):
+        """Tensor-core forward of raw inputs: (outputs [n][4], in-hull flags [n])."""
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, 3)
+        Y = np.empty((len(X), 4), dtype=np.float32)
+        hull = np.empty(len(X), dtype=np.int32)
+        check(lib().fg_surrogate_predict(self._h, _fptr(X), len(X), _fptr(Y), hull.ctypes.data_as(L.PI)))
+        return Y, hull.astype(bool)
+
+    def close(self) -> None:
+        if self._h:
+            lib().fg_surrogate_destroy(self._h)
             self._h = None
 
     def __del__(self):

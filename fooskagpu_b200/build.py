@@ -45,7 +45,8 @@ def _run(cmd, cwd=None):
 
 
 def build_product(force: bool = False, verbose: bool = False, out: Path = None, defines=()) -> Path:
-    cu = [CSRC / "fg_kernels.cu", CSRC / "fg_relax.cu", CSRC / "fg_solver.cu", CSRC / "fg_noalloc.cu"]
+    cu = [CSRC / "fg_kernels.cu", CSRC / "fg_relax.cu", CSRC / "fg_solver.cu", CSRC / "fg_noalloc.cu",
+          CSRC / "fg_surrogate.cu"]
     cpp = [CSRC / "fg_mesh.cpp"]
     hdr = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "fooskagpu.h"]
     lib_out = out or LIB

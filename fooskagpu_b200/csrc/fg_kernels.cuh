@@ -114,9 +114,17 @@ struct RelaxParams {
     double avfMin, chemLimit, thermUrf, chemUrf, satTempUrf;
     int thermItrMax, chemItrMax, chemFlag;
 };
+struct SurrogateDev;
+// optional log of chemical Newton solves (training data for the surrogate): X [cap][3], Y [cap][4]
+struct RelaxLog {
+    float *X;
+    float *Y;
+    unsigned long long *count;   // null: logging off
+    long long cap;
+};
 template <typename T>
 void launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
-                  cudaStream_t s);
+                  const SurrogateDev &S, const RelaxLog &L, cudaStream_t s);
 
 // conservation integral: blockSum then ordered final sum into out
 void launch_cons(int n, int ivar, const double *U, const double *vol, double *blockSum, double *out, cudaStream_t s);

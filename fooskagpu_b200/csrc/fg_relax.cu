@@ -5,7 +5,13 @@
 // (cells are independent, so the result is identical and deterministic).
 // Every Newton loop is bounded by the reference's iteration caps (thermItrMax, chemItrMax,
 // 50 for the saturation temperature, urf > 0.0005 for step halving).
+//
+// With a surrogate attached, a chemical cell inside the network's training hull starts from the
+// network's equilibrium prediction and takes at most `polishIters` full Newton steps on the
+// reference's residuals; it is accepted when every relative residual is within `relTol`,
+// otherwise (and outside the hull) the cell takes the reference Newton unchanged.
 #include "fg_kernels.cuh"
+#include "fg_surrogate.cuh"
 
 namespace fg {
 
@@ -262,18 +268,108 @@ __device__ int chem_cell(const RelaxParams &R, const Ph *h, double *U, int *iter
     return aborted;
 }
 
+// mixture density and internal energy per unit volume exactly as chem_cell forms them
+__device__ __forceinline__ void chem_mixture(const RelaxParams &R, const double *U, double *rm, double *re, double *ag) {
+    const double a0 = fmin(fmax(R.avfMin / 100, U[0]), 1 - R.avfMin / 100);
+    const double a1 = 1 - a0;
+    const double r0 = U[1] / a0, r1 = U[2] / a1;
+    const double m = a0 * r0 + a1 * r1;
+    const double u = U[3] / m, v = U[4] / m, w = U[5] / m;
+    *rm = m;
+    *re = U[8] - 0.5 * m * (u * u + v * v + w * w);
+    *ag = a1 * r1;
+}
+
+// Full-step Newton from the surrogate's equilibrium (p, T, alpha) on the residuals of chem_res.
+// Returns 1 and writes U when every relative residual is within relTol.
+__device__ int chem_polish(const RelaxParams &R, const Ph *h, double *U, const float *y, double rm, double re,
+                           double relTol, int maxIt, int *iters) {
+    const double p = y[0], T = y[1];
+    if (!(T > 0) || !(p > -h[0].pinf) || !(p > -h[1].pinf)) return 0;
+    double x[6];
+    const double rL = (p + h[0].pinf) / ((h[0].cp / h[0].g) * (h[0].g - 1) * T);
+    const double rG = (p + h[1].pinf) / ((h[1].cp / h[1].g) * (h[1].g - 1) * T);
+    double a = (rm - rG) / (rL - rG);   // mass balance at (p, T)
+    if (!(a > 0 && a < 1)) a = y[2];
+    if (!(a > 0 && a < 1)) return 0;
+    x[0] = a;
+    x[1] = 1 - a;
+    x[2] = rL;
+    x[3] = rG;
+    x[4] = (p + h[0].g * h[0].pinf) / ((h[0].g - 1) * rL) + h[0].eta;
+    x[5] = (p + h[1].g * h[1].pinf) / ((h[1].g - 1) * rG) + h[1].eta;
+    const int pm = (x[1] > x[0]) ? 1 : 0, mm = 1 - pm;
+    const double sp = fmax(fabs(p), 1.0), sT = T, sg = h[0].cp * T;
+    int ok = 0;
+    for (int itr = 0; itr <= maxIt; itr++) {
+        double res[3];
+        chem_res(R, h, pm, x, rm, re, res);
+        if (!(x[0] > 0 && x[0] < 1 && x[2] > 0 && x[3] > 0)) break;
+        if (fabs(res[0]) <= relTol * sp && fabs(res[1]) <= relTol * sT && fabs(res[2]) <= relTol * sg) {
+            ok = 1;
+            break;
+        }
+        if (itr == maxIt) break;
+        *iters = itr + 1;
+        const int js[3] = {mm, mm + 2, mm + 4};
+        double jac[3][3], e[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const int j = js[q];
+            e[q] = fabs(x[j]) < 1e-9 ? 1e-10 : 1.e-5 * x[j];
+            x[j] += e[q];
+            double rr[3];
+            chem_res(R, h, pm, x, rm, re, rr);
+            x[j] -= e[q];
+#pragma unroll
+            for (int i = 0; i < 3; i++) jac[i][q] = (rr[i] - res[i]) / e[q];
+        }
+        const double det = jac[0][0] * (jac[1][1] * jac[2][2] - jac[1][2] * jac[2][1]) -
+                           jac[0][1] * (jac[1][0] * jac[2][2] - jac[1][2] * jac[2][0]) +
+                           jac[0][2] * (jac[1][0] * jac[2][1] - jac[1][1] * jac[2][0]);
+        if (!(fabs(det) > 0) || !isfinite(det)) break;
+        const double id = 1.0 / det;
+        double inv[3][3];
+        inv[0][0] = id * (jac[1][1] * jac[2][2] - jac[1][2] * jac[2][1]);
+        inv[0][1] = -id * (jac[0][1] * jac[2][2] - jac[0][2] * jac[2][1]);
+        inv[0][2] = id * (jac[0][1] * jac[1][2] - jac[0][2] * jac[1][1]);
+        inv[1][0] = -id * (jac[1][0] * jac[2][2] - jac[1][2] * jac[2][0]);
+        inv[1][1] = id * (jac[0][0] * jac[2][2] - jac[0][2] * jac[2][0]);
+        inv[1][2] = -id * (jac[0][0] * jac[1][2] - jac[0][2] * jac[1][0]);
+        inv[2][0] = id * (jac[1][0] * jac[2][1] - jac[1][1] * jac[2][0]);
+        inv[2][1] = -id * (jac[0][0] * jac[2][1] - jac[0][1] * jac[2][0]);
+        inv[2][2] = id * (jac[0][0] * jac[1][1] - jac[0][1] * jac[1][0]);
+#pragma unroll
+        for (int q = 0; q < 3; q++) x[js[q]] -= inv[q][0] * res[0] + inv[q][1] * res[1] + inv[q][2] * res[2];
+    }
+    if (!ok) return 0;
+    U[0] = fmin(fmax(R.avfMin / 100, x[0]), 1 - R.avfMin / 100);
+    U[1] = x[0] * x[2];
+    U[2] = x[1] * x[3];
+    U[6] = x[0] * x[2] * x[4];
+    U[7] = x[1] * x[3] * x[5];
+    U[9] = x[1] * x[3];
+    return 1;
+}
+
 }  // namespace
 
-template <typename T>
-__global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R, int32_t *counters) {
+// kSG / kLog: instantiated with the surrogate path / the solve log; the plain instantiation
+// carries none of their code (and none of their registers)
+template <typename T, bool kSG, bool kLog>
+__global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R,
+                                               int32_t *counters, const SurrogateDev S, const RelaxLog Lg) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    int chem = 0, ab = 0, its = 0;
+    int chem = 0, ab = 0, its = 0, used = 0;
     const bool act = c < n;
+    const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
+    double u[NV];
+    double rm = 0, re = 0, ag = 0;
+    float z[3] = {0.f, 0.f, 0.f};
+    bool want = false;
     if (act) {
-        double u[NV];
 #pragma unroll
         for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
-        const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
         if (R.chemFlag == 1) {
             const double avf = fmin(fmax(R.avfMin / 100, u[0]), 1 - R.avfMin / 100);
             const double rho = u[1] / avf;
@@ -283,7 +379,47 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
             const double ts = sat_temp(R, pl, tl, R.satTempUrf);
             chem = (tl > ts && avf > R.chemLimit);
         }
-        ab = chem ? chem_cell(R, h, u, &its) : therm_cell(R, h, u, &its);
+        if (chem && (kSG || kLog)) {
+            chem_mixture(R, u, &rm, &re, &ag);
+            if (kSG) {
+                const float f[3] = {(float)rm, (float)(re / rm), (float)(ag / rm)};
+#pragma unroll
+                for (int k = 0; k < 3; k++) z[k] = (f[k] - S.norm.xMean[k]) / S.norm.xStd[k];
+                want = sg_in_hull(S.norm, z);
+            }
+        }
+    }
+    // the network runs once per warp that has a candidate cell (all 32 lanes take part)
+    float pred[4] = {0.f, 0.f, 0.f, 0.f};
+    if (kSG && __any_sync(0xffffffffu, want)) {
+        float o[4];
+        sg_warp_forward(S, z, o);
+#pragma unroll
+        for (int k = 0; k < 4; k++) pred[k] = S.norm.yMean[k] + S.norm.yStd[k] * o[k];
+    }
+    if (act) {
+        int pits = 0;
+        if (kSG && want) used = chem_polish(R, h, u, pred, rm, re, S.relTol, S.polishIters, &pits);
+        if (!used) {
+            ab = chem ? chem_cell(R, h, u, &its) : therm_cell(R, h, u, &its);
+            if (kLog && chem && !ab) {
+                // training sample: (rho, e, Y) before the solve -> (p, T, alpha, Y_eq) after it
+                const unsigned long long k = atomicAdd(Lg.count, 1ULL);
+                if (k < (unsigned long long)Lg.cap) {
+                    const double a0 = fmin(fmax(R.avfMin / 100, u[0]), 1 - R.avfMin / 100);
+                    const double rL = u[1] / a0, eL = u[6] / u[1];
+                    float *x = Lg.X + k * 3, *y = Lg.Y + k * 4;
+                    x[0] = (float)rm;
+                    x[1] = (float)(re / rm);
+                    x[2] = (float)(ag / rm);
+                    y[0] = (float)p_of(h[0], rL, eL);
+                    y[1] = (float)t_of(h[0], rL, eL);
+                    y[2] = (float)a0;
+                    y[3] = (float)(u[9] / rm);
+                }
+            }
+        }
+        its += pits;   // polish steps count as Newton iterations (accepted or not)
         U[(size_t)0 * n + c] = u[0];
         U[(size_t)1 * n + c] = u[1];
         U[(size_t)2 * n + c] = u[2];
@@ -302,21 +438,33 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
     const unsigned mask = __ballot_sync(0xffffffffu, act && chem);
     const unsigned maskT = __ballot_sync(0xffffffffu, act && !chem);
     const unsigned maskA = __ballot_sync(0xffffffffu, act && ab);
+    const unsigned maskS = __ballot_sync(0xffffffffu, act && used);
+    const unsigned maskF = __ballot_sync(0xffffffffu, act && chem && kSG && !used);
     const int itsW = __reduce_add_sync(0xffffffffu, its);
     if ((threadIdx.x & 31) == 0) {
         if (maskT) atomicAdd(&counters[0], __popc(maskT));
         if (mask) atomicAdd(&counters[1], __popc(mask));
         if (maskA) atomicAdd(&counters[2], __popc(maskA));
         if (itsW) atomicAdd(&counters[3], itsW);
+        if (maskS) atomicAdd(&counters[4], __popc(maskS));
+        if (maskF) atomicAdd(&counters[5], __popc(maskF));
     }
 }
 
 template <typename T>
-void launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters, cudaStream_t s) {
-    k_relax<T><<<(n + 127) / 128, 128, 0, s>>>(n, U, W, D, R, counters);
+void launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
+                  const SurrogateDev &S, const RelaxLog &L, cudaStream_t s) {
+    const int nb = (n + 127) / 128;
+    const bool lg = L.count != nullptr;
+    if (S.enabled && lg) k_relax<T, true, true><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L);
+    else if (S.enabled) k_relax<T, true, false><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L);
+    else if (lg) k_relax<T, false, true><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L);
+    else k_relax<T, false, false><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L);
 }
 
-template void launch_relax<float>(int, double *, float *, const PhysD &, const RelaxParams &, int32_t *, cudaStream_t);
-template void launch_relax<double>(int, double *, double *, const PhysD &, const RelaxParams &, int32_t *, cudaStream_t);
+template void launch_relax<float>(int, double *, float *, const PhysD &, const RelaxParams &, int32_t *,
+                                  const SurrogateDev &, const RelaxLog &, cudaStream_t);
+template void launch_relax<double>(int, double *, double *, const PhysD &, const RelaxParams &, int32_t *,
+                                   const SurrogateDev &, const RelaxLog &, cudaStream_t);
 
 }  // namespace fg

@@ -4,6 +4,7 @@
 #include "../../include/fooskagpu.h"
 #include "fg_kernels.cuh"
 #include "fg_mesh.h"
+#include "fg_surrogate.cuh"
 
 #include <climits>
 #include <cmath>
@@ -39,10 +40,17 @@ int set_err(int code, const std::string &msg) {
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
-    ~DevBuf() {
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
         if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
     }
     cudaError_t alloc(size_t b) {
+        release();
         bytes = b;
         return cudaMalloc(&p, b ? b : 16);
     }
@@ -51,6 +59,11 @@ struct DevBuf {
 };
 
 }  // namespace
+
+namespace fg {
+int surrogate_view(const fg_surrogate *g, SurrogateDev *out);
+int surrogate_device(const fg_surrogate *g);
+}  // namespace fg
 
 // ------------------------------------------------------------------ solver base
 struct fg_solver {
@@ -99,6 +112,12 @@ struct fg_solver {
         recKind.clear();
     }
     fg_case cs{};
+    // attached equilibrium surrogate (not owned) and the optional chemical-solve log
+    const fg_surrogate *sg = nullptr;
+    double sgTol = 1e-6;
+    int sgIters = 3;
+    DevBuf logX, logY, logCnt;
+    long long logCap = 0;
     int n = 0, nSlots = 0;
     int iStep = 0;
     uint64_t bytes = 0;
@@ -111,6 +130,7 @@ struct fg_solver {
     virtual int update(int irk, int writeU0, cudaStream_t s) = 0;
     virtual int stage(int irk, int writeU0, cudaStream_t s) = 0;
     virtual int relax(fg_relax_stats *st, cudaStream_t s) = 0;
+    virtual int relax_counts(fg_relax_stats *st) = 0;
     virtual int cons(int ivar, double *out, cudaStream_t s) = 0;
     virtual int advance_time(cudaStream_t s) = 0;
     virtual int get_time(double *dt, double *t) = 0;
@@ -388,7 +408,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dSig.alloc((size_t)n * sizeof(double)));
         FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n), cons_blocks(n)) * sizeof(double)));
         FG_CUDA_TRY(dScal.alloc(4 * sizeof(double)));   // dt, time, cons
-        FG_CUDA_TRY(dCnt.alloc(4 * sizeof(int32_t)));
+        FG_CUDA_TRY(dCnt.alloc(8 * sizeof(int32_t)));
         FG_CUDA_TRY(cudaMemset(dU.p, 0, u));
         FG_CUDA_TRY(cudaMemset(dU0.p, 0, u));
         FG_CUDA_TRY(cudaMemset(dRHS.p, 0, u));
@@ -519,20 +539,35 @@ struct SolverT : public fg_solver {
         return FG_OK;
     }
     int relax(fg_relax_stats *st, cudaStream_t s) override {
-        FG_CUDA_TRY(cudaMemsetAsync(dCnt.p, 0, 4 * sizeof(int32_t), s));
+        FG_CUDA_TRY(cudaMemsetAsync(dCnt.p, 0, 8 * sizeof(int32_t), s));
+        SurrogateDev S{};
+        if (sg) {
+            const int rc = surrogate_view(sg, &S);
+            if (rc != FG_OK) return rc;
+            S.relTol = sgTol;
+            S.polishIters = sgIters;
+        }
+        RelaxLog L{logX.as<float>(), logY.as<float>(), logCap > 0 ? logCnt.as<unsigned long long>() : nullptr, logCap};
         prof_begin(FG_K_RELAX, s);
-        launch_relax<T>(n, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), s);
+        launch_relax<T>(n, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), S, L, s);
         prof_end(s);
         FG_LAUNCH_CHECK("relaxation");
         if (st) {
-            int32_t h[4];
-            FG_CUDA_TRY(cudaMemcpyAsync(h, dCnt.p, sizeof(h), cudaMemcpyDeviceToHost, s));
             FG_CUDA_TRY(cudaStreamSynchronize(s));
-            st->nTherm = h[0];
-            st->nChem = h[1];
-            st->nAbort = h[2];
-            st->nIter = h[3];
+            return relax_counts(st);
         }
+        return FG_OK;
+    }
+    int relax_counts(fg_relax_stats *st) override {
+        int32_t h[8];
+        FG_CUDA_TRY(cudaDeviceSynchronize());
+        FG_CUDA_TRY(cudaMemcpy(h, dCnt.p, sizeof(h), cudaMemcpyDeviceToHost));
+        st->nTherm = h[0];
+        st->nChem = h[1];
+        st->nAbort = h[2];
+        st->nIter = h[3];
+        st->nSurrogate = h[4];
+        st->nFallback = h[5];
         return FG_OK;
     }
     int cons(int ivar, double *out, cudaStream_t s) override {
@@ -805,6 +840,60 @@ int fg_stage(fg_solver *s, int32_t irk, void *stream) {
 int fg_relaxation(fg_solver *s, fg_relax_stats *stats, void *stream) {
     FG_ENTER(s);
     return s->relax(stats, (cudaStream_t)stream);
+}
+int fg_solver_set_surrogate(fg_solver *s, const fg_surrogate *g, double relTol, int32_t polishIters) {
+    FG_ENTER(s);
+    if (g) {
+        if (!(relTol > 0) || polishIters < 0 || polishIters > 20)
+            return set_err(FG_ERR_ARG, "fg_solver_set_surrogate: relTol > 0 and 0 <= polishIters <= 20");
+        if (fg::surrogate_device(g) != s->device)
+            return set_err(FG_ERR_ARG, "fg_solver_set_surrogate: surrogate lives on another device");
+        fg::SurrogateDev tmp{};
+        const int rc = fg::surrogate_view(g, &tmp);
+        if (rc != FG_OK) return rc;
+    }
+    s->sg = g;
+    s->sgTol = relTol;
+    s->sgIters = polishIters;
+    return FG_OK;
+}
+int fg_relax_stats_read(fg_solver *s, fg_relax_stats *stats) {
+    FG_ENTER(s);
+    if (!stats) return set_err(FG_ERR_ARG, "fg_relax_stats_read: null argument");
+    return s->relax_counts(stats);
+}
+int fg_relax_log(fg_solver *s, int64_t capacity) {
+    FG_ENTER(s);
+    if (capacity < 0 || capacity > ((int64_t)1 << 31)) return set_err(FG_ERR_ARG, "fg_relax_log: 0 <= capacity <= 2^31");
+    s->logX.release();
+    s->logY.release();
+    s->logCnt.release();
+    s->logCap = 0;
+    if (capacity == 0) return FG_OK;
+    FG_CUDA_TRY(s->logX.alloc((size_t)capacity * 3 * sizeof(float)));
+    FG_CUDA_TRY(s->logY.alloc((size_t)capacity * 4 * sizeof(float)));
+    FG_CUDA_TRY(s->logCnt.alloc(sizeof(unsigned long long)));
+    FG_CUDA_TRY(cudaMemset(s->logCnt.p, 0, sizeof(unsigned long long)));
+    s->logCap = capacity;
+    return FG_OK;
+}
+int fg_relax_log_read(fg_solver *s, float *X, float *Y, int64_t cap, int64_t *count) {
+    FG_ENTER(s);
+    if (!count) return set_err(FG_ERR_ARG, "fg_relax_log_read: null count");
+    *count = 0;
+    if (s->logCap == 0) return FG_OK;
+    unsigned long long c = 0;
+    FG_CUDA_TRY(cudaDeviceSynchronize());
+    FG_CUDA_TRY(cudaMemcpy(&c, s->logCnt.p, sizeof(c), cudaMemcpyDeviceToHost));
+    const int64_t have = std::min<int64_t>((int64_t)c, s->logCap);
+    const int64_t k = std::min<int64_t>(have, cap);
+    if (k > 0) {
+        if (!X || !Y) return set_err(FG_ERR_ARG, "fg_relax_log_read: null buffer");
+        FG_CUDA_TRY(cudaMemcpy(X, s->logX.p, (size_t)k * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+        FG_CUDA_TRY(cudaMemcpy(Y, s->logY.p, (size_t)k * 4 * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    *count = k;
+    return FG_OK;
 }
 int fg_cons_calc(fg_solver *s, int32_t ivar, double *out, void *stream) {
     FG_ENTER(s);

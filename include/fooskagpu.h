@@ -209,9 +209,51 @@ typedef struct fg_relax_stats {
     int32_t nTherm;       /* cells relaxed thermally          */
     int32_t nChem;        /* cells relaxed chemically         */
     int32_t nAbort;       /* Newton solves that fell back to the best iterate */
-    int32_t nIter;        /* Newton iterations summed over all cells */
+    int32_t nIter;        /* Newton iterations summed over all cells (surrogate polish steps included) */
+    int32_t nSurrogate;   /* chemical cells solved from the surrogate's prediction            */
+    int32_t nFallback;    /* chemical cells that took the reference Newton with a surrogate attached
+                             (outside the training hull, or polish residual above tolerance)   */
 } fg_relax_stats;
 int fg_relaxation(fg_solver *s, fg_relax_stats *stats, void *stream);
+/* counts of the most recent relaxation, including the one inside fg_step (synchronises) */
+int fg_relax_stats_read(fg_solver *s, fg_relax_stats *stats);
+
+/* ---------------------------------------------------------------- learned equilibrium surrogate
+ * No counterpart in the reference (whose chemical relaxation is the per-cell Newton of
+ * DP/chemRlx.cu:4-267).  An MLP 3 -> 64 -> 64 -> 64 -> 4 (GELU) maps a chemical cell's
+ * (rho, e, Y) — mixture density, mixture internal energy per unit mass, vapour mass fraction
+ * before the solve — to the equilibrium (p, T, alpha, Y_eq).  Trained on the GPU (FP32, Adam)
+ * on samples logged from the solver's own Newton solves; evaluated in the relaxation kernel on
+ * the BF16 tensor cores (FP32 accumulation).  The prediction seeds at most polishIters full
+ * Newton steps on the reference's residuals; a cell is accepted when |p_L - p_G| <= relTol |p|,
+ * |T_L - T_G| <= relTol T and |g_L - g_G| <= relTol Cp_L T, else (and for inputs outside the
+ * training hull: per-feature box plus a Mahalanobis bound) it takes the reference Newton. */
+typedef struct fg_surrogate fg_surrogate;
+#define FG_SG_NPARAM 8836   /* W1[3][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64][4] b4[4] */
+#define FG_SG_NNORM 30      /* xMean[3] xStd[3] yMean[4] yStd[4] boxLo[3] boxHi[3] covInv[9] d2Max */
+int fg_surrogate_create(int32_t device, uint64_t seed, fg_surrogate **out);   /* seeded random init */
+int fg_surrogate_destroy(fg_surrogate *g);
+/* X [n][3] = (rho, e, Y), Y [n][4] = (p, T, alpha, Y_eq), host FP32; sets the standardisation and
+ * the training hull from these samples and keeps them on the device for training */
+int fg_surrogate_set_data(fg_surrogate *g, const float *X, const float *Y, int64_t n);
+/* epochs of shuffled mini-batches (Adam, cosine-decayed lr); *final_loss = loss of the last batch */
+int fg_surrogate_train(fg_surrogate *g, int32_t epochs, int32_t batch, float lr, uint64_t seed, float *final_loss);
+/* mean squared error over the 4 outputs of n standardised samples and its gradient [FG_SG_NPARAM]
+ * (FP32 forward/backward kernels, no update); host arrays */
+int fg_surrogate_loss_grad(fg_surrogate *g, const float *Xs, const float *Ys, int32_t n, float *loss, float *grad);
+int fg_surrogate_get_params(fg_surrogate *g, float *params);
+int fg_surrogate_set_params(fg_surrogate *g, const float *params);
+int fg_surrogate_get_norm(fg_surrogate *g, float *norm);
+int fg_surrogate_set_norm(fg_surrogate *g, const float *norm);
+/* tensor-core forward of n raw inputs (host arrays): Y [n][4] raw outputs, in_hull [n] (may be NULL) */
+int fg_surrogate_predict(fg_surrogate *g, const float *X, int32_t n, float *Y, int32_t *in_hull);
+/* attach (g != NULL) or detach the surrogate used by fg_relaxation / fg_step; g must outlive the
+ * attachment and live on the solver's device */
+int fg_solver_set_surrogate(fg_solver *s, const fg_surrogate *g, double relTol, int32_t polishIters);
+/* log of chemical Newton solves as surrogate training samples: capacity 0 turns it off;
+ * fg_relax_log_read copies min(logged, cap) samples (X [][3], Y [][4], order not defined) */
+int fg_relax_log(fg_solver *s, int64_t capacity);
+int fg_relax_log_read(fg_solver *s, float *X, float *Y, int64_t cap, int64_t *count);
 
 /* consCalc (DP/consCalc.cu:40): FP64 integral of variable ivar over the domain
  * (ivar 0 integrates 1-alpha).  Deterministic two-level reduction. */
