@@ -122,9 +122,19 @@ struct RelaxLog {
     unsigned long long *count;   // null: logging off
     long long cap;
 };
+// work arrays of the chemical-first cell ordering (n bytes + 4 n + 8 nb + 4 bytes)
+struct RelaxOrder {
+    uint8_t *isChem;     // [n]
+    int32_t *blockCnt;   // [relax_order_blocks(n)]
+    int32_t *blockOff;   // [relax_order_blocks(n)]
+    int32_t *order;      // [n]
+    int32_t *total;      // [1] chemical cells
+};
+int relax_order_blocks(int n);
+// returns the number of kernels launched
 template <typename T>
-void launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
-                  const SurrogateDev &S, const RelaxLog &L, cudaStream_t s);
+int launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
+                 const SurrogateDev &S, const RelaxLog &L, const RelaxOrder &O, cudaStream_t s);
 
 // conservation integral: blockSum then ordered final sum into out
 void launch_cons(int n, int ivar, const double *U, const double *vol, double *blockSum, double *out, cudaStream_t s);

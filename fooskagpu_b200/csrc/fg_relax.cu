@@ -352,16 +352,99 @@ __device__ int chem_polish(const RelaxParams &R, const Ph *h, double *U, const f
     return 1;
 }
 
+// partitionRelaxation (DP/relaxation.cu:4-75): the cell needs the chemical (Gibbs) solve when its
+// liquid temperature is above the saturation temperature at its liquid pressure and its
+// volume fraction above chemLimit
+__device__ __forceinline__ int needs_chem(const RelaxParams &R, const Ph *h, const double *u) {
+    const double avf = fmin(fmax(R.avfMin / 100, u[0]), 1 - R.avfMin / 100);
+    const double rho = u[1] / avf;
+    const double enr = u[6] / (avf * rho);
+    const double tl = t_of(h[0], rho, enr);
+    const double pl = p_of(h[0], rho, enr);
+    const double ts = sat_temp(R, pl, tl, R.satTempUrf);
+    return (tl > ts && avf > R.chemLimit);
+}
+
 }  // namespace
 
-// kSG / kLog: instantiated with the surrogate path / the solve log; the plain instantiation
-// carries none of their code (and none of their registers)
-template <typename T, bool kSG, bool kLog>
-__global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R,
-                                               int32_t *counters, const SurrogateDev S, const RelaxLog Lg) {
+// ---- ordering of the cells for the relaxation: chemical cells first, then thermal cells, each
+// in cell order (a deterministic block prefix sum; no atomics), so that every warp of the
+// relaxation kernel but one runs a single branch
+constexpr int kOrdThreads = 256;
+
+__global__ void k_relax_partition(int n, const double *__restrict__ U, const RelaxParams R, uint8_t *isChem,
+                                  int32_t *blockChem) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int chem = 0;
+    if (c < n) {
+        const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
+        double u[NV];
+        u[0] = U[c];
+        u[1] = U[(size_t)n + c];
+        u[6] = U[(size_t)6 * n + c];
+        chem = needs_chem(R, h, u);
+        isChem[c] = (uint8_t)chem;
+    }
+    const int cnt = __syncthreads_count(chem);
+    if (threadIdx.x == 0) blockChem[blockIdx.x] = cnt;
+}
+
+// exclusive scan of the per-block counts (one block of 1024 threads), total into *total
+__global__ void k_relax_scan(const int32_t *cnt, int nb, int32_t *off, int32_t *total) {
+    __shared__ int32_t sh[1024];
+    const int t = threadIdx.x;
+    const int per = (nb + 1023) / 1024;
+    const int lo = min(nb, t * per), hi = min(nb, lo + per);
+    int s = 0;
+    for (int i = lo; i < hi; i++) s += cnt[i];
+    sh[t] = s;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+        const int v = (t >= d) ? sh[t - d] : 0;
+        __syncthreads();
+        sh[t] += v;
+        __syncthreads();
+    }
+    int base = t ? sh[t - 1] : 0;
+    for (int i = lo; i < hi; i++) {
+        off[i] = base;
+        base += cnt[i];
+    }
+    if (t == 1023) *total = sh[1023];
+}
+
+__global__ void k_relax_order(int n, const uint8_t *isChem, const int32_t *blockOff, const int32_t *total,
+                              int32_t *order) {
+    __shared__ int32_t warpChem[kOrdThreads / 32];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int chem = (c < n) ? isChem[c] : 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, chem);
+    if (lane == 0) warpChem[wid] = __popc(bal);
+    __syncthreads();
+    int before = 0;   // chemical cells of this block before this warp
+    for (int w = 0; w < wid; w++) before += warpChem[w];
+    if (c >= n) return;
+    const int rankC = before + __popc(bal & ((1u << lane) - 1u));    // chemical cells before c in the block
+    const int rankT = (int)threadIdx.x - rankC;                       // thermal cells before c in the block
+    const int b = blockIdx.x;
+    if (chem) order[blockOff[b] + rankC] = c;
+    else order[*total + (b * kOrdThreads - blockOff[b]) + rankT] = c;
+}
+
+
+// kSG / kLog: instantiated with the surrogate path / the solve log; the plain instantiation
+// carries none of their code (and none of their registers).  kOrd: thread i relaxes cell
+// order[i], chemical when i < *nChem (k_relax_order); otherwise thread i relaxes cell i and
+// decides the branch itself.
+template <typename T, bool kSG, bool kLog, bool kOrd>
+__global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R,
+                                               int32_t *counters, const SurrogateDev S, const RelaxLog Lg,
+                                               const int32_t *order, const int32_t *nChem) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool act = i < n;
+    const int c = (kOrd && act) ? order[i] : i;
     int chem = 0, ab = 0, its = 0, used = 0;
-    const bool act = c < n;
     const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
     double u[NV];
     double rm = 0, re = 0, ag = 0;
@@ -370,15 +453,7 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
     if (act) {
 #pragma unroll
         for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
-        if (R.chemFlag == 1) {
-            const double avf = fmin(fmax(R.avfMin / 100, u[0]), 1 - R.avfMin / 100);
-            const double rho = u[1] / avf;
-            const double enr = u[6] / (avf * rho);
-            const double tl = t_of(h[0], rho, enr);
-            const double pl = p_of(h[0], rho, enr);
-            const double ts = sat_temp(R, pl, tl, R.satTempUrf);
-            chem = (tl > ts && avf > R.chemLimit);
-        }
+        if (R.chemFlag == 1) chem = kOrd ? (i < *nChem) : needs_chem(R, h, u);
         if (chem && (kSG || kLog)) {
             chem_mixture(R, u, &rm, &re, &ag);
             if (kSG) {
@@ -451,20 +526,39 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
     }
 }
 
-template <typename T>
-void launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
-                  const SurrogateDev &S, const RelaxLog &L, cudaStream_t s) {
+int relax_order_blocks(int n) { return (n + kOrdThreads - 1) / kOrdThreads; }
+
+template <typename T, bool kOrd>
+static void launch_relax_k(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
+                           const SurrogateDev &S, const RelaxLog &L, const int32_t *order, const int32_t *nChem,
+                           cudaStream_t s) {
     const int nb = (n + 127) / 128;
     const bool lg = L.count != nullptr;
-    if (S.enabled && lg) k_relax<T, true, true><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L);
-    else if (S.enabled) k_relax<T, true, false><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L);
-    else if (lg) k_relax<T, false, true><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L);
-    else k_relax<T, false, false><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L);
+    if (S.enabled && lg) k_relax<T, true, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem);
+    else if (S.enabled) k_relax<T, true, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem);
+    else if (lg) k_relax<T, false, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem);
+    else k_relax<T, false, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem);
 }
 
-template void launch_relax<float>(int, double *, float *, const PhysD &, const RelaxParams &, int32_t *,
-                                  const SurrogateDev &, const RelaxLog &, cudaStream_t);
-template void launch_relax<double>(int, double *, double *, const PhysD &, const RelaxParams &, int32_t *,
-                                   const SurrogateDev &, const RelaxLog &, cudaStream_t);
+template <typename T>
+int launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
+                 const SurrogateDev &S, const RelaxLog &L, const RelaxOrder &O, cudaStream_t s) {
+    if (R.chemFlag != 1) {
+        // every cell is thermal: no ordering needed
+        launch_relax_k<T, false>(n, U, W, D, R, counters, S, L, nullptr, nullptr, s);
+        return 1;
+    }
+    const int nb = relax_order_blocks(n);
+    k_relax_partition<<<nb, kOrdThreads, 0, s>>>(n, U, R, O.isChem, O.blockCnt);
+    k_relax_scan<<<1, 1024, 0, s>>>(O.blockCnt, nb, O.blockOff, O.total);
+    k_relax_order<<<nb, kOrdThreads, 0, s>>>(n, O.isChem, O.blockOff, O.total, O.order);
+    launch_relax_k<T, true>(n, U, W, D, R, counters, S, L, O.order, O.total, s);
+    return 4;
+}
+
+template int launch_relax<float>(int, double *, float *, const PhysD &, const RelaxParams &, int32_t *,
+                                 const SurrogateDev &, const RelaxLog &, const RelaxOrder &, cudaStream_t);
+template int launch_relax<double>(int, double *, double *, const PhysD &, const RelaxParams &, int32_t *,
+                                  const SurrogateDev &, const RelaxLog &, const RelaxOrder &, cudaStream_t);
 
 }  // namespace fg

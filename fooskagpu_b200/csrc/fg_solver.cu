@@ -149,6 +149,7 @@ struct SolverT : public fg_solver {
     DevBuf dNbr, dFlags, dGeo, dVol, dVolP, dNew2Old, dHaloStart, dHaloIds, dSlotLocal;
     DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dBlockMin, dScal, dCnt, dCons, dStage;
     DevBuf dFIdx, dFGeo, dSlotFace, dClosure, dFB;
+    DevBuf dOrdFlag, dOrdCnt, dOrdOff, dOrder, dOrdTotal;   // relaxation cell ordering
     int cur = 0;
     DevMesh<T> dm{};
     PhysT<T> P{};
@@ -409,6 +410,11 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n), cons_blocks(n)) * sizeof(double)));
         FG_CUDA_TRY(dScal.alloc(4 * sizeof(double)));   // dt, time, cons
         FG_CUDA_TRY(dCnt.alloc(8 * sizeof(int32_t)));
+        FG_CUDA_TRY(dOrdFlag.alloc((size_t)n));
+        FG_CUDA_TRY(dOrdCnt.alloc((size_t)relax_order_blocks(n) * sizeof(int32_t)));
+        FG_CUDA_TRY(dOrdOff.alloc((size_t)relax_order_blocks(n) * sizeof(int32_t)));
+        FG_CUDA_TRY(dOrder.alloc((size_t)n * sizeof(int32_t)));
+        FG_CUDA_TRY(dOrdTotal.alloc(sizeof(int32_t)));
         FG_CUDA_TRY(cudaMemset(dU.p, 0, u));
         FG_CUDA_TRY(cudaMemset(dU0.p, 0, u));
         FG_CUDA_TRY(cudaMemset(dRHS.p, 0, u));
@@ -420,7 +426,7 @@ struct SolverT : public fg_solver {
         bytes = 0;
         for (DevBuf *b : {&dNbr, &dFlags, &dGeo, &dVol, &dVolP, &dNew2Old, &dU, &dU0, &dRHS, &dStage, &dW[0], &dW[1], &dG,
                           &dSig, &dBlockMin, &dScal, &dCnt, &dHaloStart, &dHaloIds, &dSlotLocal, &dFIdx, &dFGeo,
-                          &dSlotFace, &dClosure, &dFB})
+                          &dSlotFace, &dClosure, &dFB, &dOrdFlag, &dOrdCnt, &dOrdOff, &dOrder, &dOrdTotal})
             bytes += b->bytes;
         dm.n = n;
         dm.nSlots = nSlots;
@@ -548,9 +554,12 @@ struct SolverT : public fg_solver {
             S.polishIters = sgIters;
         }
         RelaxLog L{logX.as<float>(), logY.as<float>(), logCap > 0 ? logCnt.as<unsigned long long>() : nullptr, logCap};
+        const RelaxOrder O{dOrdFlag.as<uint8_t>(), dOrdCnt.as<int32_t>(), dOrdOff.as<int32_t>(), dOrder.as<int32_t>(),
+                           dOrdTotal.as<int32_t>()};
         prof_begin(FG_K_RELAX, s);
-        launch_relax<T>(n, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), S, L, s);
+        const int k = launch_relax<T>(n, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), S, L, O, s);
         prof_end(s);
+        launches += k - 1;
         FG_LAUNCH_CHECK("relaxation");
         if (st) {
             FG_CUDA_TRY(cudaStreamSynchronize(s));
