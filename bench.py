@@ -120,6 +120,23 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def rank_max(x: float, dist, device) -> float:
+    """Max of a per-rank time over all ranks (replicas: each rank times its own copy of the
+    workload; the slowest rank sets the whole job's time)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world: int, cells: int, stages: int, steps: int, ms_max: float) -> float:
+    """Whole-job cell-updates/s of `world` replicas that each ran `steps` steps of `cells` cells
+    with `stages` RK stages, the slowest taking ms_max."""
+    return world * cells * stages * steps / (ms_max / 1e3)
+
+
 def time_steps(solver, steps: int, torch, stream):
     """Device time of `steps` fg_step calls on `stream` (CUDA events)."""
     e0 = torch.cuda.Event(enable_timing=True)
@@ -157,11 +174,7 @@ def run_ours(args, rank, world, local_rank, dist):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, dist, f"cuda:{dev}")
 
     # ---------------- mixed path: headline value
     s = Solver(mesh, case, precision="mixed", device=dev)
@@ -178,7 +191,7 @@ def run_ours(args, rank, world, local_rank, dist):
     barrier()
     launches = s.launch_count() - n0
     ms = max_over_ranks(ms)
-    value = world * nE * rk * args.steps / (ms / 1e3)
+    value = job_value(world, nE, rk, args.steps, ms)
     # per-kernel CUDA-event times over a second timed region of the same length
     s.profile(True)
     time_steps(s, args.steps, torch, stream)
@@ -204,7 +217,7 @@ def run_ours(args, rank, world, local_rank, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_val = world * nE * rk * e2e_steps / (e2e_ms / 1e3)
+    e2e_val = job_value(world, nE, rk, e2e_steps, e2e_ms)
     s.close()
 
     # ---------------- FP64 path on the same workload
@@ -215,7 +228,7 @@ def run_ours(args, rank, world, local_rank, dist):
     k64 = max(3, args.steps // 2)
     barrier()
     ms64 = max_over_ranks(time_steps(s64, k64, torch, stream))
-    fp64_value = world * nE * rk * k64 / (ms64 / 1e3)
+    fp64_value = job_value(world, nE, rk, k64, ms64)
     s64.profile(True)
     time_steps(s64, k64, torch, stream)
     prof64 = s64.profile_read()

@@ -118,7 +118,7 @@ def test_tensor_core_forward_matches_oracle(trained, data):
 def test_training_reduces_loss(trained):
     g, loss0, loss = trained
     _report("surrogate/train", dict(initial=loss0, final=loss))
-    assert loss < 1e-3 * loss0 and loss < 1e-3, (loss0, loss)
+    assert loss < 2e-3 * loss0 and loss < 5e-3, (loss0, loss)
 
 
 def test_relaxation_gain_and_parity(box, trained):
