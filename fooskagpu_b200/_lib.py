@@ -106,6 +106,9 @@ SIGNATURES = {
     "fg_surrogate_predict": (C.c_int, [VP, PF, i32, PF, PI]),
     "fg_solver_set_surrogate": (C.c_int, [VP, VP, f64, i32]),
     "fg_relax_log": (C.c_int, [VP, i64]),
+    "fg_checkpoint_write": (C.c_int, [VP, C.c_char_p]),
+    "fg_checkpoint_read": (C.c_int, [VP, C.c_char_p]),
+    "fg_field_dump": (C.c_int, [VP, C.c_char_p]),
     "fg_relax_stats_read": (C.c_int, [VP, C.POINTER(FgRelaxStats)]),
     "fg_relax_log_read": (C.c_int, [VP, PF, PF, i64, C.POINTER(i64)]),
     "fg_get_time": (C.c_int, [VP, PD, PD, PI]),

@@ -141,6 +141,16 @@ class Solver:
         return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter,
                 "nSurrogate": st.nSurrogate, "nFallback": st.nFallback}
 
+    # -- checkpoint / restart and field output
+    def checkpoint_write(self, path: str) -> None:
+        check(lib().fg_checkpoint_write(self._h, str(path).encode()))
+
+    def checkpoint_read(self, path: str) -> None:
+        check(lib().fg_checkpoint_read(self._h, str(path).encode()))
+
+    def field_dump(self, path: str) -> None:
+        check(lib().fg_field_dump(self._h, str(path).encode()))
+
     def relax_stats(self) -> dict:
         """Counts of the most recent relaxation (also the one inside step())."""
         st = FgRelaxStats()
@@ -300,3 +310,17 @@ class Surrogate:
             self.close()
         except Exception:
             pass
+
+
+FIELD_VARS = ["x", "y", "z", "avfL", "avfG", "rho", "U", "V", "W", "pressure", "temperature", "vaporMass", "gradRho"]
+
+
+def read_field_dump(path: str) -> dict:
+    """Read a field dump written by Solver.field_dump: {"time", "iStep", "data" [nElem][13], "names"}."""
+    raw = open(path, "rb").read()
+    if raw[:8] != b"FGFIELD1":
+        raise ValueError(f"{path}: not a field dump")
+    n, nv, istep, _ = np.frombuffer(raw, dtype=np.int32, count=4, offset=8)
+    t = float(np.frombuffer(raw, dtype=np.float64, count=1, offset=24)[0])
+    data = np.frombuffer(raw, dtype=np.float64, count=int(n) * int(nv), offset=32).reshape(int(n), int(nv))
+    return {"time": t, "iStep": int(istep), "data": data.copy(), "names": FIELD_VARS[: int(nv)]}

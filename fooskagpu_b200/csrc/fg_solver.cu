@@ -112,6 +112,8 @@ struct fg_solver {
         recKind.clear();
     }
     fg_case cs{};
+    int precision = FG_PREC_FP64;
+    std::vector<double> cellCenter;   // reference order, for the field dump
     // attached equilibrium surrogate (not owned) and the optional chemical-solve log
     const fg_surrogate *sg = nullptr;
     double sgTol = 1e-6;
@@ -135,6 +137,9 @@ struct fg_solver {
     virtual int advance_time(cudaStream_t s) = 0;
     virtual int get_time(double *dt, double *t) = 0;
     virtual int set_dt(double dt) = 0;
+    virtual int set_time(double t) = 0;
+    // 13 export variables per cell in .neu element order (host array nElem * 13)
+    virtual int field_vars(double *out) = 0;
     virtual int get_rhs(double *rhs) = 0;
     virtual int get_limited(double *grad, double *theta) = 0;
     virtual int get_signal(double *sig) = 0;
@@ -143,6 +148,43 @@ struct fg_solver {
 namespace fg {
 
 __global__ void k_advance_time(const double *dt, double *t) { *t += *dt; }
+
+// export variables of DP/export_plt.cu:42-80 per cell (not averaged to the nodes): x y z avfL avfG
+// rho U V W pressure temperature vaporMass |grad rho|, the last from the most recent gradient
+// pass; written to out[old * 13 + k] (the .neu element order)
+template <typename T>
+__global__ void k_field_vars(int n, const double *__restrict__ U, const T *__restrict__ G, const int32_t *new2old,
+                             const PhysD D, const double *cp, double *out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    double u[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
+    const double aL = u[0], aG = 1 - aL;
+    const double rL = u[1] / aL, rG = u[2] / aG;
+    const double rho = aL * rL + aG * rG;
+    const double eL = u[6] / (aL * rL), eG = u[7] / (aG * rG);
+    const double pL = D.gm1[0] * rL * eL - D.gpinf[0] - D.gm1eta[0] * rL;
+    const double pG = D.gm1[1] * rG * eG - D.gpinf[1] - D.gm1eta[1] * rG;
+    const double tL = (pL + D.pinf[0]) / ((cp[0] / D.gam[0]) * D.gm1[0] * rL);
+    const double tG = (pG + D.pinf[1]) / ((cp[1] / D.gam[1]) * D.gm1[1] * rG);
+    // grad rho = (rhoL - rhoG) grad alpha + alpha grad rhoL + (1 - alpha) grad rhoG
+    const T *g = G + (size_t)c * GREC + NP;   // gradients of W: var v at g[3 v + d]
+    double gr[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) gr[d] = (rL - rG) * (double)g[d] + aL * (double)g[3 + d] + aG * (double)g[6 + d];
+    double *o = out + (size_t)new2old[c] * 13;
+    o[3] = aL;
+    o[4] = aG;
+    o[5] = rho;
+    o[6] = u[3] / rho;
+    o[7] = u[4] / rho;
+    o[8] = u[5] / rho;
+    o[9] = aL * pL + aG * pG;
+    o[10] = aL * tL + aG * tG;
+    o[11] = u[9];
+    o[12] = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+}
 
 template <typename T>
 struct SolverT : public fg_solver {
@@ -174,6 +216,7 @@ struct SolverT : public fg_solver {
     int init(const fg::Mesh &m) override {
         n = m.nElem;
         nSlots = m.maxFaces;
+        cellCenter.assign(m.cellCenter.begin(), m.cellCenter.end());
         // physics constants in T and FP64
         for (int k = 0; k < 2; k++) {
             const double g = cs.gamma[k];
@@ -612,6 +655,24 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(cudaMemcpy(dScal.p, &dt, sizeof(double), cudaMemcpyHostToDevice));
         return FG_OK;
     }
+    int set_time(double t) override {
+        FG_CUDA_TRY(cudaDeviceSynchronize());
+        FG_CUDA_TRY(cudaMemcpy(dScal.as<double>() + 1, &t, sizeof(double), cudaMemcpyHostToDevice));
+        return FG_OK;
+    }
+    int field_vars(double *out) override {
+        DevBuf dOut, dCp;
+        FG_CUDA_TRY(dOut.alloc((size_t)n * 13 * sizeof(double)));
+        FG_CUDA_TRY(dCp.alloc(2 * sizeof(double)));
+        FG_CUDA_TRY(cudaMemcpy(dCp.p, cs.Cp, 2 * sizeof(double), cudaMemcpyHostToDevice));
+        k_field_vars<T><<<(n + 255) / 256, 256>>>(n, dU.as<double>(), dG.as<T>(), dNew2Old.as<int32_t>(), D,
+                                                  dCp.as<double>(), dOut.as<double>());
+        FG_LAUNCH_CHECK("field_vars");
+        launches++;
+        FG_CUDA_TRY(cudaDeviceSynchronize());
+        FG_CUDA_TRY(cudaMemcpy(out, dOut.p, (size_t)n * 13 * sizeof(double), cudaMemcpyDeviceToHost));
+        return FG_OK;
+    }
     int get_rhs(double *rhs) override {
         launch_gather_state(n, dRHS.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), 0);
         FG_LAUNCH_CHECK("get_rhs");
@@ -785,6 +846,7 @@ int fg_solver_create(const fg_mesh *m, const fg_case *c, int32_t precision, int3
     std::unique_ptr<fg_solver> s;
     if (precision == FG_PREC_FP64) s.reset(new fg::SolverT<double>());
     else if (precision == FG_PREC_MIXED) s.reset(new fg::SolverT<float>());
+    if (s) s->precision = precision;
     else return set_err(FG_ERR_ARG, "unknown precision");
     s->device = device;
     s->cs = *c;
@@ -917,6 +979,84 @@ int fg_get_time(fg_solver *s, double *dt, double *physicalTime, int32_t *iStep) 
 int fg_set_dt(fg_solver *s, double dt) {
     FG_ENTER(s);
     return s->set_dt(dt);
+}
+
+// ---- checkpoint / restart and field dump (binary; the reference writes ASCII with 11 digits,
+// DP/restart.cu:113-152, and node-averaged Tecplot text, DP/export_plt.cu:95-174)
+namespace {
+const char kCkMagic[8] = {'F', 'G', 'C', 'K', 'P', 'T', '0', '1'};
+const char kFdMagic[8] = {'F', 'G', 'F', 'I', 'E', 'L', 'D', '1'};
+struct CkHeader {
+    char magic[8];
+    int32_t nElem, neq, iStep, precision;
+    double physicalTime, dt;
+};
+}  // namespace
+
+int fg_checkpoint_write(fg_solver *s, const char *path) {
+    FG_ENTER(s);
+    if (!path) return set_err(FG_ERR_ARG, "fg_checkpoint_write: null path");
+    std::vector<double> U((size_t)s->n * fg::NV);
+    int rc = s->get_state(U.data(), 0);
+    if (rc != FG_OK) return rc;
+    CkHeader h{};
+    std::memcpy(h.magic, kCkMagic, 8);
+    h.nElem = s->n;
+    h.neq = fg::NV;
+    h.iStep = s->iStep;
+    h.precision = s->precision;
+    rc = s->get_time(&h.dt, &h.physicalTime);
+    if (rc != FG_OK) return rc;
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return set_err(FG_ERR_IO, std::string("fg_checkpoint_write: cannot open ") + path);
+    const bool ok = fwrite(&h, sizeof(h), 1, fp) == 1 && fwrite(U.data(), sizeof(double), U.size(), fp) == U.size();
+    if (fclose(fp) != 0 || !ok) return set_err(FG_ERR_IO, std::string("fg_checkpoint_write: write failed: ") + path);
+    return FG_OK;
+}
+
+int fg_checkpoint_read(fg_solver *s, const char *path) {
+    FG_ENTER(s);
+    if (!path) return set_err(FG_ERR_ARG, "fg_checkpoint_read: null path");
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return set_err(FG_ERR_IO, std::string("fg_checkpoint_read: cannot open ") + path);
+    CkHeader h{};
+    std::vector<double> U((size_t)s->n * fg::NV);
+    bool ok = fread(&h, sizeof(h), 1, fp) == 1 && std::memcmp(h.magic, kCkMagic, 8) == 0;
+    if (ok && (h.nElem != s->n || h.neq != fg::NV)) {
+        fclose(fp);
+        return set_err(FG_ERR_ARG, "fg_checkpoint_read: checkpoint is for " + std::to_string(h.nElem) +
+                                       " cells, the solver has " + std::to_string(s->n));
+    }
+    ok = ok && fread(U.data(), sizeof(double), U.size(), fp) == U.size();
+    fclose(fp);
+    if (!ok) return set_err(FG_ERR_IO, std::string("fg_checkpoint_read: not a checkpoint or truncated: ") + path);
+    int rc = s->set_state(U.data(), 0);
+    if (rc == FG_OK) rc = s->set_dt(h.dt);
+    if (rc == FG_OK) rc = s->set_time(h.physicalTime);
+    if (rc != FG_OK) return rc;
+    s->iStep = h.iStep;
+    return FG_OK;
+}
+
+int fg_field_dump(fg_solver *s, const char *path) {
+    FG_ENTER(s);
+    if (!path) return set_err(FG_ERR_ARG, "fg_field_dump: null path");
+    const double *cellCenter = s->cellCenter.data();
+    std::vector<double> v((size_t)s->n * 13);
+    int rc = s->field_vars(v.data());
+    if (rc != FG_OK) return rc;
+    for (int i = 0; i < s->n; i++)
+        for (int d = 0; d < 3; d++) v[(size_t)i * 13 + d] = cellCenter[(size_t)i * 3 + d];
+    double t = 0, dt = 0;
+    rc = s->get_time(&dt, &t);
+    if (rc != FG_OK) return rc;
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return set_err(FG_ERR_IO, std::string("fg_field_dump: cannot open ") + path);
+    const int32_t hdr[4] = {s->n, 13, s->iStep, 0};
+    const bool ok = fwrite(kFdMagic, 1, 8, fp) == 8 && fwrite(hdr, sizeof(hdr), 1, fp) == 1 &&
+                    fwrite(&t, sizeof(double), 1, fp) == 1 && fwrite(v.data(), sizeof(double), v.size(), fp) == v.size();
+    if (fclose(fp) != 0 || !ok) return set_err(FG_ERR_IO, std::string("fg_field_dump: write failed: ") + path);
+    return FG_OK;
 }
 
 int fg_step(fg_solver *s, void *stream) {

@@ -279,6 +279,21 @@ int fg_cons_integral_noalloc(const double *U, const double *vol, int32_t nCells,
 int fg_get_time(fg_solver *s, double *dt, double *physicalTime, int32_t *iStep);
 int fg_set_dt(fg_solver *s, double dt);
 
+/* Checkpoint / restart (DP/restart.cu:113-152 writeFieldRestart, :424-497 readField, which store
+ * consVec as 11-digit ASCII).  Binary and exact: header (magic "FGCKPT01", nElem, NEQ, iStep,
+ * precision, physicalTime, dt) + U[nElem*10] in .neu element order.  fg_checkpoint_read restores
+ * the state, dt, physical time and step counter; restarting reproduces an uninterrupted run
+ * bit for bit. */
+int fg_checkpoint_write(fg_solver *s, const char *path);
+int fg_checkpoint_read(fg_solver *s, const char *path);
+
+/* Field dump replacing the Tecplot ASCII export (DP/export_plt.cu:95-174): binary, per cell in
+ * .neu element order (not averaged to the nodes): magic "FGFIELD1", int32 {nElem, 13, iStep, 0},
+ * double physicalTime, then double[nElem][13] = x y z avfL avfG rho U V W pressure temperature
+ * vaporMass |grad rho| (pressure and temperature volume-fraction weighted as the reference's
+ * export; |grad rho| from the most recent gradient pass). */
+int fg_field_dump(fg_solver *s, const char *path);
+
 /* One explicitLoop iteration (DP/explicitLoop.cu:28-64): time advance, RK stages with the
  * adaptive dt at stage 0 every adaptDtItr steps, relaxation, conservation every adaptDtItr. */
 int fg_step(fg_solver *s, void *stream);
