@@ -41,7 +41,8 @@ class FgCase(C.Structure):
         ("satTempUrf", f64),
         ("pInf", f64 * 2), ("gamma", f64 * 2), ("Cp", f64 * 2), ("eta", f64 * 2), ("satConst", f64 * 2),
         ("dynVisc", f64 * 2), ("heatCoef", f64 * 2), ("Pr", f64 * 2),
-        ("relaxFlag", i32), ("hllcEnergyFix", i32), ("hllcTieTol", f64), ("reserved", i32 * 4),
+        ("relaxFlag", i32), ("hllcEnergyFix", i32), ("hllcTieTol", f64), ("heatFlux", i32),
+        ("reserved", i32 * 3),
     ]
 
 

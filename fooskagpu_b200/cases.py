@@ -86,9 +86,14 @@ def sod_ic(case: FgCase, centres: np.ndarray, x0: float = 0.5, alpha: float = 0.
     return prim_to_cons(case, alpha, rho, rho, z, z, z, p)
 
 
-def tgv_case(mach=0.1, re=1600.0, rk=3, cfl=0.5) -> FgCase:
-    """Taylor-Green vortex, rho0 = V0 = L = 1, mu = rho0 V0 L / Re, WALE LES."""
-    return ideal_gas_case(gamma=1.4, cp=3.5, mu=1.0 / re, rk=rk, cfl=cfl, adapt_itr=100)
+def tgv_case(mach=0.1, re=1600.0, rk=3, cfl=0.5, pr=0.71) -> FgCase:
+    """Taylor-Green vortex, rho0 = V0 = L = 1, mu = rho0 V0 L / Re, WALE LES, heat conduction at
+    Prandtl number pr (the heat-flux extension; pr = 0 turns it off)."""
+    c = ideal_gas_case(gamma=1.4, cp=3.5, mu=1.0 / re, rk=rk, cfl=cfl, adapt_itr=100)
+    if pr > 0:
+        c.heatFlux = 1
+        c.Pr[0] = c.Pr[1] = pr
+    return c
 
 
 def tgv_ic(case: FgCase, centres: np.ndarray, mach=0.1, alpha: float = 0.5) -> np.ndarray:

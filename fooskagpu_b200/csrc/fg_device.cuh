@@ -30,7 +30,8 @@ struct PhysT {
     // inlet ghost state (DP/bc.h:2-25), precomputed in FP64 on the host
     T inAlpha, inRhoL, inRhoG, inP;
     T tieTol;      // |S*| <= tieTol (|S_L| + |S_R|) counts as S* = 0 (extension; 0 = reference)
-    int woods, visc, turb, energyFix;
+    T cp[2], prn[2];   // heat conduction (extension): k = cp mu / Pr
+    int woods, visc, turb, energyFix, heat;
 };
 
 struct PhysD {

@@ -308,6 +308,17 @@ __device__ __forceinline__ void face_state(const T *w, const T *g, T dx, T dy, T
     }
 }
 
+// gradient of the liquid-phase temperature T = (p_L + pInf) / (cv (gamma - 1) rho_L) of a cell from
+// its record and gradients (chain rule), added to acc
+template <typename T>
+__device__ __forceinline__ void cell_grad_t(const PhysT<T> &P, const T *w, const T *g, T *acc) {
+    const T rl = w[1], pl = w[6];
+    const T c = (pl + P.pinf[0]) / rl;
+    const T inv = (T)1 / (P.cvgm1[0] * rl);
+#pragma unroll
+    for (int d = 0; d < 3; d++) acc[d] += (g[NP + 3 * 6 + d] - c * g[NP + 3 * 1 + d]) * inv;
+}
+
 // ------------------------------------------------------------------ face flux (once per face)
 // Record of face f with canonical normal n (owner -> neighbour), area A:
 //   H[v] = A (F[v] - Visc[v]) + A pF n (momentum),  u = A (u* . n),  signal
@@ -326,6 +337,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::face) k_face(const DevMesh<
     const int nb = m.fNb[fi];
     const T nx = m.fnx[fi], ny = m.fny[fi], nz = m.fnz[fi], A = m.fA[fi];
     T wo[NP], sL[NP], sR[NP], p1[NP], gO[9], gN[9];
+    T gT[3] = {0, 0, 0};   // sum of the two cells' temperature gradients (heat conduction)
     {
         T g[GREC];
         load_rec(W, o, wo);
@@ -333,6 +345,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::face) k_face(const DevMesh<
         face_state(wo, g, m.fdo[0][fi], m.fdo[1][fi], m.fdo[2][fi], sL);
 #pragma unroll
         for (int q = 0; q < 9; q++) gO[q] = g[NP + 9 + q];
+        if (P.heat && nb >= 0) cell_grad_t(P, wo, g, gT);
     }
     if (nb >= 0) {
         T wn[NP], g[GREC];
@@ -341,6 +354,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::face) k_face(const DevMesh<
         face_state(wn, g, m.fdn[0][fi], m.fdn[1][fi], m.fdn[2][fi], sR);
 #pragma unroll
         for (int q = 0; q < 9; q++) gN[q] = g[NP + 9 + q];
+        if (P.heat) cell_grad_t(P, wn, g, gT);
 #pragma unroll
         for (int v = 0; v < NP; v++) p1[v] = sR[v];
     } else {
@@ -383,6 +397,12 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::face) k_face(const DevMesh<
         H[5] -= muA * (t02 * nx + t12 * ny + t22 * nz);
         H[8] -= muA * ((t00 * vx + t01 * vy + t02 * vz) * nx + (t01 * vx + t11 * vy + t12 * vz) * ny +
                        (t02 * vx + t12 * vy + t22 * vz) * nz);
+        if (P.heat && nb >= 0) {
+            // Fourier conduction k grad T . n (extension); adiabatic boundary faces
+            const T aF = (a1 + a2) * (T)0.5;
+            const T kF = mu * (aF * P.cp[0] + (1 - aF) * P.cp[1]) / (aF * P.prn[0] + (1 - aF) * P.prn[1]);
+            H[8] -= A * kF * (T)0.5 * (gT[0] * nx + gT[1] * ny + gT[2] * nz);
+        }
     }
     T sig = 0;
     if (wantSignal) {

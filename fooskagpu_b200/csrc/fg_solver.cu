@@ -228,6 +228,8 @@ struct SolverT : public fg_solver {
             P.cvgm1[k] = (T)((cs.Cp[k] / g) * (g - 1));
             P.gm1eta[k] = (T)((g - 1) * cs.eta[k]);
             P.mu[k] = (T)cs.dynVisc[k];
+            P.cp[k] = (T)cs.Cp[k];
+            P.prn[k] = (T)cs.Pr[k];
             D.gam[k] = g;
             D.gm1[k] = g - 1;
             D.pinf[k] = cs.pInf[k];
@@ -245,6 +247,9 @@ struct SolverT : public fg_solver {
         P.chemLimit = (T)cs.chemLimit;
         P.woods = (cs.woodsFlag == 1);
         P.visc = (cs.viscFlag == 1);
+        P.heat = (cs.viscFlag == 1 && cs.heatFlux == 1);
+        if (P.heat && !(cs.Pr[0] > 0 && cs.Pr[1] > 0))
+            return set_err(FG_ERR_ARG, "heatFlux needs Pr[0] > 0 and Pr[1] > 0");
         P.turb = (cs.turbulence == 1);
         P.energyFix = (cs.hllcEnergyFix == 1);
         P.tieTol = (T)cs.hllcTieTol;

@@ -105,7 +105,13 @@ typedef struct fg_case {
      *   makes two implementations with different rounding take the same branch. */
     int32_t hllcEnergyFix;
     double  hllcTieTol;
-    int32_t reserved[4];
+    /* heatFlux = 1 (with viscFlag = 1): Fourier heat conduction in the viscous energy flux,
+     * k = cp mu / Pr with cp, Pr volume-fraction weighted at the face and mu the viscous flux's
+     * (laminar + WALE), temperature gradient = mean of the two cells' liquid-phase
+     * T = (p + pInf) / (cv (gamma - 1) rho) gradients; adiabatic boundary faces.  The reference
+     * declares Pr and heatCoef (DP/strdata.h:96-97) but never uses them. */
+    int32_t heatFlux;
+    int32_t reserved[3];
 } fg_case;
 
 /* Fill *c with the values the reference hard-codes in DP/buildInput.cu:10-69. */

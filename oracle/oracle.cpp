@@ -320,10 +320,22 @@ double eddy_visc(double ux, double uy, double uz, double vx, double vy, double v
     return Ls * Ls * num / den;
 }
 
-/* Viscous face flux (DP/computeViscousStresses.cu:66-174) — out[0..9] owner, [10..19] nb. */
+/* Gradient of the liquid-phase temperature T = (pL + pInf) / (cv (gamma - 1) rhoL) of a cell
+ * (chain rule on the gradients of rhoL and pL), for the heat-conduction extension. */
+static void cell_grad_t(const fg_case *c, const double *U, const double *g, double *out) {
+    double s[10];
+    cons2prim(c, U, s);
+    const double rl = s[1], pl = s[6];
+    const double cvgm1 = (c->Cp[0] / c->gamma[0]) * (c->gamma[0] - 1);
+    const double k = (pl + c->pInf[0]) / rl;
+    for (int d = 0; d < 3; d++) out[d] = (g[6 * 3 + d] - k * g[1 * 3 + d]) / (cvgm1 * rl);
+}
+
+/* Viscous face flux (DP/computeViscousStresses.cu:66-174) — out[0..9] owner, [10..19] nb.
+ * Uo / Un: cell-centre states of owner and neighbour (heat-conduction extension only). */
 void viscous_face(const fg_case *c, const double *gO, const double *gN, double volAvg,
                   const double *pf0, const double *pf1, const double *n, double A, int bc,
-                  double *out) {
+                  const double *Uo, const double *Un, double *out) {
     const double ux = (gO[9 + 0] + gN[9 + 0]) / 2, uy = (gO[9 + 1] + gN[9 + 1]) / 2, uz = (gO[9 + 2] + gN[9 + 2]) / 2;
     const double vx = (gO[12 + 0] + gN[12 + 0]) / 2, vy = (gO[12 + 1] + gN[12 + 1]) / 2, vz = (gO[12 + 2] + gN[12 + 2]) / 2;
     const double wx = (gO[15 + 0] + gN[15 + 0]) / 2, wy = (gO[15 + 1] + gN[15 + 1]) / 2, wz = (gO[15 + 2] + gN[15 + 2]) / 2;
@@ -362,6 +374,20 @@ void viscous_face(const fg_case *c, const double *gO, const double *gN, double v
     }
     out[8] = (fe[0] + fe[1] + fe[2]) * A;
     if (bc == 0) out[18] = -(fe[0] + fe[1] + fe[2]) * A;
+    if (c->heatFlux == 1 && bc == 0) {
+        /* Fourier conduction (extension): k = cp mu / Pr at the face, mean of the two cells'
+         * temperature gradients; boundary faces adiabatic */
+        double tO[3], tN[3];
+        cell_grad_t(c, Uo, gO, tO);
+        cell_grad_t(c, Un, gN, tN);
+        const double cpF = aF * c->Cp[0] + (1 - aF) * c->Cp[1];
+        const double prF = aF * c->Pr[0] + (1 - aF) * c->Pr[1];
+        const double kF = mu * cpF / prF;
+        double q = 0;
+        for (int d = 0; d < 3; d++) q += 0.5 * (tO[d] + tN[d]) * n[d];
+        out[8] += kF * q * A;
+        out[18] -= kF * q * A;
+    }
 }
 
 /* Max signal speed of a face state (DP/computeTimeStep.cu:15-46). */
@@ -950,7 +976,7 @@ void orc_rhs(const fg_case *c, const fg_mesh_view *m, const double *U, orc_work 
             } else {
                 const double vavg = (m->volume[o] + m->volume[nb]) / 2;
                 viscous_face(c, w->grad + (size_t)o * 30, w->grad + (size_t)nb * 30, vavg, pf, pf + 10, n,
-                             m->area[f], bc, fb + (size_t)f * 20);
+                             m->area[f], bc, U + (size_t)o * 10, U + (size_t)nb * 10, fb + (size_t)f * 20);
             }
         }
 #pragma omp parallel for num_threads(g_threads) schedule(static)

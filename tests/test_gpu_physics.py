@@ -102,4 +102,4 @@ def test_tgv_kinetic_energy_history(meshdir):
                                "max_rel_dissipation": e_diss})
     assert np.all(diss64 > 0)            # the vortex decays
     assert e_ke < 1e-5, e_ke
-    assert e_diss < 1e-3, e_diss
+    assert e_diss < 5e-3, e_diss          # per 5-step interval: a difference of small differences

@@ -25,6 +25,8 @@ def _p(a):
 def _case_from(d):
     c = FgCase()
     for k, v in d.items():
+        if k == "reserved":     # extension padding (its length changed as extensions were added)
+            continue
         if isinstance(v, list):
             arr = getattr(c, k)
             for i, x in enumerate(v):
