@@ -42,7 +42,7 @@ class FgCase(C.Structure):
         ("pInf", f64 * 2), ("gamma", f64 * 2), ("Cp", f64 * 2), ("eta", f64 * 2), ("satConst", f64 * 2),
         ("dynVisc", f64 * 2), ("heatCoef", f64 * 2), ("Pr", f64 * 2),
         ("relaxFlag", i32), ("hllcEnergyFix", i32), ("hllcTieTol", f64), ("heatFlux", i32),
-        ("reserved", i32 * 3),
+        ("limiter", i32), ("inletVelFlag", i32), ("reserved", i32 * 3), ("inletVel", f64 * 3),
     ]
 
 

@@ -31,7 +31,8 @@ struct PhysT {
     T inAlpha, inRhoL, inRhoG, inP;
     T tieTol;      // |S*| <= tieTol (|S_L| + |S_R|) counts as S* = 0 (extension; 0 = reference)
     T cp[2], prn[2];   // heat conduction (extension): k = cp mu / Pr
-    int woods, visc, turb, energyFix, heat;
+    T inVel[3];        // prescribed inlet velocity (extension, inVelFlag)
+    int woods, visc, turb, energyFix, heat, limiter, inVelFlag;
 };
 
 struct PhysD {
@@ -93,6 +94,11 @@ __device__ __forceinline__ void ghost_state(const PhysT<T> &P, int bc, T nx, T n
         s[6] = P.inP;
         s[7] = P.inP;
         s[8] = 0;
+        if (P.inVelFlag) {
+            s[3] = P.inVel[0];
+            s[4] = P.inVel[1];
+            s[5] = P.inVel[2];
+        }
     }
 }
 

@@ -200,7 +200,8 @@ __device__ __forceinline__ void stage_geometry(const DevMesh<T> &m, int lo, int 
 }
 
 // ------------------------------------------------------------------ gradient + limiter
-template <typename T>
+// kLim: 0 the reference's limiter function, 1 the van Albada-type extension (fg_case.limiter)
+template <typename T, int kLim>
 __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_grad(const DevMesh<T> m, const T *__restrict__ W,
                                                                 T *__restrict__ G, const PhysT<T> P) {
     constexpr int WS = Stage<T>::WS;
@@ -286,7 +287,15 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
             const T wun = w[v] + ext;
             const T diff = wun - w[v];
             T phi = 1;
-            if (diff != 0) phi = ((wun > w[v]) ? (mx[v] - w[v]) : (mn[v] - w[v])) / (2 * diff);
+            if (diff != 0) {
+                if (kLim == 1) {
+                    // van Albada-type limiter function (extension)
+                    const T r = ((wun > w[v]) ? (mx[v] - w[v]) : (mn[v] - w[v])) / diff;
+                    phi = (r * r + r) / (r * r + 1);
+                } else {
+                    phi = ((wun > w[v]) ? (mx[v] - w[v]) : (mn[v] - w[v])) / (2 * diff);
+                }
+            }
             th[v] = fmin(th[v], fmax((T)0, fmin(phi, (T)1)));
         }
     }
@@ -634,14 +643,18 @@ static size_t grad_smem(const DevMesh<T> &m) {
 }
 template <typename T>
 int stage_kernels_setup(const DevMesh<T> &m) {
-    if (cudaFuncSetAttribute(k_grad<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem(m)) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_grad<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem(m)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_grad<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem(m)) != cudaSuccess)
         return 1;
     return 0;
 }
 template <typename T>
 void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cudaStream_t s) {
     const int nb = (m.n + m.blockCells - 1) / m.blockCells;
-    k_grad<T><<<nb, m.blockCells, grad_smem(m), s>>>(m, f.Win, f.G, P);
+    if (P.limiter == 1)
+        k_grad<T, 1><<<nb, m.blockCells, grad_smem(m), s>>>(m, f.Win, f.G, P);
+    else
+        k_grad<T, 0><<<nb, m.blockCells, grad_smem(m), s>>>(m, f.Win, f.G, P);
 }
 template <typename T>
 void launch_face(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, int wantSignal, cudaStream_t s) {

@@ -248,6 +248,10 @@ struct SolverT : public fg_solver {
         P.woods = (cs.woodsFlag == 1);
         P.visc = (cs.viscFlag == 1);
         P.heat = (cs.viscFlag == 1 && cs.heatFlux == 1);
+        P.limiter = cs.limiter;
+        P.inVelFlag = (cs.inletVelFlag == 1);
+        for (int d = 0; d < 3; d++) P.inVel[d] = (T)cs.inletVel[d];
+        if (cs.limiter != 0 && cs.limiter != 1) return set_err(FG_ERR_UNSUPPORTED, "limiter must be 0 or 1");
         if (P.heat && !(cs.Pr[0] > 0 && cs.Pr[1] > 0))
             return set_err(FG_ERR_ARG, "heatFlux needs Pr[0] > 0 and Pr[1] > 0");
         P.turb = (cs.turbulence == 1);

@@ -111,7 +111,15 @@ typedef struct fg_case {
      * T = (p + pInf) / (cv (gamma - 1) rho) gradients; adiabatic boundary faces.  The reference
      * declares Pr and heatCoef (DP/strdata.h:96-97) but never uses them. */
     int32_t heatFlux;
+    /* limiter = 1: van Albada-type limiter function phi(r) = min(1, (r^2 + r) / (r^2 + 1)) with
+     * r = (w_max - w) / Delta (or w_min), in place of the reference's phi = r / 2
+     * (DP/computeFaceValues.cu:73-79), the minimum over the cell's faces as before. */
+    int32_t limiter;
+    /* inletVelFlag = 1: the inlet ghost (bc 3) takes the velocity inletVel instead of the
+     * interior velocity (the reference's inlet copies it, DP/bc.h:8-18). */
+    int32_t inletVelFlag;
     int32_t reserved[3];
+    double  inletVel[3];
 } fg_case;
 
 /* Fill *c with the values the reference hard-codes in DP/buildInput.cu:10-69. */

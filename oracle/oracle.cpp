@@ -156,6 +156,11 @@ void bc_values(const fg_case *c, const double *n, const double *t1, const double
         s[7] = pIn;
         s[8] = 0;
         s[9] = 0;
+        if (c->inletVelFlag == 1) {   /* prescribed inlet velocity (extension) */
+            s[3] = c->inletVel[0];
+            s[4] = c->inletVel[1];
+            s[5] = c->inletVel[2];
+        }
     }
     /* bc == 2 (outlet): zero gradient, ghost = interior */
 }
@@ -891,7 +896,7 @@ void orc_grad(const fg_case *, const fg_mesh_view *m, orc_work *w) {
 }
 
 /* initializeTheta + computeLimiter + updateFaces (DP/computeFaceValues.cu:4-113) */
-void orc_limiter(const fg_case *, const fg_mesh_view *m, orc_work *w) {
+void orc_limiter(const fg_case *c, const fg_mesh_view *m, orc_work *w) {
     orc_work_ext *e = ext_of(w, m);
     const int nE = m->nElem, nF = m->nFcs;
     /* extension and per-side limiter value, face-parallel */
@@ -932,10 +937,16 @@ void orc_limiter(const fg_case *, const fg_mesh_view *m, orc_work *w) {
                 const double wun = sol + (xf - xc) * g[0] + (yf - yc) * g[1] + (zf - zc) * g[2];
                 const double wmax = w->wMax[(size_t)cI * 10 + v], wmin = w->wMin[(size_t)cI * 10 + v];
                 double phi;
-                if (wun - sol != 0)
-                    phi = (wun > sol) ? (wmax - sol) / (2 * (wun - sol)) : (wmin - sol) / (2 * (wun - sol));
-                else
+                if (wun - sol != 0) {
+                    if (c->limiter == 1) {   /* van Albada-type limiter function (extension) */
+                        const double r = (wun > sol) ? (wmax - sol) / (wun - sol) : (wmin - sol) / (wun - sol);
+                        phi = (r * r + r) / (r * r + 1);
+                    } else {
+                        phi = (wun > sol) ? (wmax - sol) / (2 * (wun - sol)) : (wmin - sol) / (2 * (wun - sol));
+                    }
+                } else {
                     phi = 1;
+                }
                 const double tt = fmax(0, fmin(phi, 1));
                 if (th[v] > tt) th[v] = tt;   /* atomic min */
             }

@@ -17,7 +17,8 @@ HERE = Path(__file__).resolve().parent
 EXE = HERE / "_ref" / "fooska_ref_dp"
 
 # case fields of ours that the reference's INPUT struct does not have
-EXTENSION_KEYS = ("relaxFlag", "hllcEnergyFix", "hllcTieTol", "heatFlux", "reserved")
+EXTENSION_KEYS = ("relaxFlag", "hllcEnergyFix", "hllcTieTol", "heatFlux", "limiter", "inletVelFlag", "reserved",
+                  "inletVel")
 
 
 def available() -> bool:

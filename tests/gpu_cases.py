@@ -23,7 +23,18 @@ def make(name: str, meshdir, prec: str = "fp64") -> tuple:
     """Return (Mesh, case, U0) for a named parity case."""
     path = os.path.join(str(meshdir), name + ".neu")
     periodic = (0.0, 0.0, 0.0)
-    if name == "tet_ref":
+    if name == "tet_ext":
+        # the extensions the configurations need: van Albada-type limiter, prescribed inlet velocity
+        path = os.path.join(str(meshdir), "tet_ref.neu")
+        if not os.path.exists(path):
+            meshgen.write_neu(path, meshgen.box_tets(6, 3, 3, L=(0.006, 0.003, 0.003), origin=(-0.003, 0, 0),
+                                                     jitter=0.1, side_bc=ALL_BC))
+        c = cases.reference_case()
+        c.limiter = 1
+        c.inletVelFlag = 1
+        c.inletVel[0], c.inletVel[1], c.inletVel[2] = 30.0, 2.0, -1.0
+        ic = "perturbed"
+    elif name == "tet_ref":
         if not os.path.exists(path):
             meshgen.write_neu(path, meshgen.box_tets(6, 3, 3, L=(0.006, 0.003, 0.003), origin=(-0.003, 0, 0),
                                                      jitter=0.1, side_bc=ALL_BC))
@@ -63,4 +74,4 @@ def make(name: str, meshdir, prec: str = "fp64") -> tuple:
     return m, c, U
 
 
-NAMES = ["tet_ref", "mixed_ref_rk3", "hex_periodic_tgv", "tet_sod"]
+NAMES = ["tet_ref", "mixed_ref_rk3", "hex_periodic_tgv", "tet_sod", "tet_ext"]

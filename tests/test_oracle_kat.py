@@ -25,7 +25,7 @@ def _p(a):
 def _case_from(d):
     c = FgCase()
     for k, v in d.items():
-        if k == "reserved":     # extension padding (its length changed as extensions were added)
+        if k == "reserved" or not hasattr(c, k):   # extension padding / fields of other versions
             continue
         if isinstance(v, list):
             arr = getattr(c, k)

@@ -45,3 +45,25 @@ def test_oracle_sod_l1(tmp_path):
     l1 = sod_l1(U, a["cellCenter"], a["volume"], 0.2)
     assert l1_0 < 1e-3           # the initial state is the exact solution at t = 0+
     assert l1 < 0.02, l1         # coarse MUSCL + HLLC on 16 mm tets
+
+
+def test_van_albada_limiter_is_less_diffusive(tmp_path):
+    """The limiter extension (van Albada-type phi) against the reference's phi = r / 2 on the same
+    tube: lower L1 error at t = 0.2."""
+    path = str(tmp_path / "sod.neu")
+    meshgen.write_neu(path, meshgen.box_tets(60, 2, 2, L=(1.0, 0.04, 0.04), jitter=0.1, side_bc=SLIP))
+    m = Mesh.load_neu(path, scale=1.0)
+    a = m.arrays()
+    l1 = {}
+    for lim in (0, 1):
+        c = cases.sod_case()
+        c.adaptDt = 0
+        c.dt = 0.002
+        c.consCalcFlag = 0
+        c.limiter = lim
+        U = cases.sod_ic(c, a["cellCenter"])
+        o = Oracle(m.view(), c)
+        for _ in range(100):
+            o.step(U)
+        l1[lim] = sod_l1(U, a["cellCenter"], a["volume"], 0.2)
+    assert l1[1] < l1[0], l1
