@@ -141,6 +141,12 @@ class Solver:
         return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter,
                 "nSurrogate": st.nSurrogate, "nFallback": st.nFallback}
 
+    def check_state(self) -> int:
+        """-1 if the state is healthy; raises FgError (FG_ERR_NAN) naming the step otherwise."""
+        k = C.c_int32()
+        check(lib().fg_check_state(self._h, C.byref(k)))
+        return k.value
+
     # -- checkpoint / restart and field output
     def checkpoint_write(self, path: str) -> None:
         check(lib().fg_checkpoint_write(self._h, str(path).encode()))

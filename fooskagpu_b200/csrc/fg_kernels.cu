@@ -496,6 +496,7 @@ __global__ void __launch_bounds__(256, MinBlocks<T>::gather) k_gather(const DevM
                 u[v] = r;
                 f.U[q] = r;
             }
+            if (!state_ok(u)) *f.bad = f.step + 1;
             T wo[NP];
             cons2prim_d(D, u, wo);
             store_rec(f.Wout, c, wo);
@@ -540,6 +541,7 @@ __global__ void k_update(const DevMesh<T> m, Fields<T> f, const PhysD D, StageCo
         u[v] = r;
         f.U[q] = r;
     }
+    if (!state_ok(u)) *f.bad = f.step + 1;
     T wo[NP];
     cons2prim_d(D, u, wo);
     store_rec(f.Wout, c, wo);

@@ -69,6 +69,19 @@ int surrogate_device(const fg_surrogate *g);
 struct fg_solver {
     virtual ~fg_solver() {
         for (cudaEvent_t e : evPool) cudaEventDestroy(e);
+        if (hBad) cudaFreeHost((void *)hBad);
+    }
+    int init_flag() {
+        void *h = nullptr;
+        FG_CUDA_TRY(cudaHostAlloc(&h, sizeof(int32_t), cudaHostAllocMapped));
+        hBad = static_cast<volatile int32_t *>(h);
+        *hBad = 0;
+        FG_CUDA_TRY(cudaHostGetDevicePointer((void **)&dBad, h, 0));
+        return FG_OK;
+    }
+    int bad_state_error() const {
+        return set_err(FG_ERR_NAN, "the state became non-finite or got a negative partial density in step " +
+                                       std::to_string(*hBad - 1) + " (reset it with fg_set_state / fg_checkpoint_read)");
     }
     int device = 0;
     // ---- instrumentation: events around every launch when enabled
@@ -113,6 +126,9 @@ struct fg_solver {
     }
     fg_case cs{};
     int precision = FG_PREC_FP64;
+    // failure flag written by the RK kernels (mapped host memory: read without a stream sync)
+    volatile int32_t *hBad = nullptr;
+    int32_t *dBad = nullptr;
     std::vector<double> cellCenter;   // reference order, for the field dump
     // attached equilibrium surrogate (not owned) and the optional chemical-solve log
     const fg_surrogate *sg = nullptr;
@@ -146,6 +162,12 @@ struct fg_solver {
 };
 
 namespace fg {
+
+inline bool state_ok_host(const double *u) {
+    double sum = 0;
+    for (int v = 0; v < NV; v++) sum += u[v];
+    return std::isfinite(sum) && u[0] >= 0.0 && u[0] <= 1.0 && u[1] >= 0.0 && u[2] >= 0.0;
+}
 
 __global__ void k_advance_time(const double *dt, double *t) { *t += *dt; }
 
@@ -210,6 +232,8 @@ struct SolverT : public fg_solver {
         f.signal = dSig.as<double>();
         f.blockMin = dBlockMin.as<double>();
         f.dt = dScal.as<double>();
+        f.bad = dBad;
+        f.step = iStep;
         return f;
     }
 
@@ -217,6 +241,8 @@ struct SolverT : public fg_solver {
         n = m.nElem;
         nSlots = m.maxFaces;
         cellCenter.assign(m.cellCenter.begin(), m.cellCenter.end());
+        FG_CUDA_TRY(cudaSetDevice(device));
+        if (init_flag() != FG_OK) return FG_ERR_CUDA;
         // physics constants in T and FP64
         for (int k = 0; k < 2; k++) {
             const double g = cs.gamma[k];
@@ -513,6 +539,14 @@ struct SolverT : public fg_solver {
     }
 
     int set_state(const double *U, cudaStream_t s) override {
+        for (int i = 0; i < n; i++) {
+            const double *u = U + (size_t)i * NV;
+            if (!state_ok_host(u))
+                return set_err(FG_ERR_NAN, "fg_set_state: cell " + std::to_string(i) +
+                                               " is not finite or has alpha outside [0, 1] or a negative partial density");
+        }
+        FG_CUDA_TRY(cudaStreamSynchronize(s));
+        *hBad = 0;
         FG_CUDA_TRY(cudaMemcpyAsync(dStage.p, U, (size_t)n * NV * sizeof(double), cudaMemcpyHostToDevice, s));
         prof_begin(FG_K_OTHER, s);
         launch_scatter_state(n, dStage.as<double>(), dNew2Old.as<int32_t>(), dU.as<double>(), s);
@@ -1068,8 +1102,16 @@ int fg_field_dump(fg_solver *s, const char *path) {
     return FG_OK;
 }
 
+int fg_check_state(fg_solver *s, int32_t *badStep) {
+    FG_ENTER(s);
+    FG_CUDA_TRY(cudaDeviceSynchronize());
+    if (badStep) *badStep = *s->hBad ? *s->hBad - 1 : -1;
+    return *s->hBad ? s->bad_state_error() : FG_OK;
+}
+
 int fg_step(fg_solver *s, void *stream) {
     FG_ENTER(s);
+    if (*s->hBad) return s->bad_state_error();
     cudaStream_t st = (cudaStream_t)stream;
     const fg_case &c = s->cs;
     int rc = s->advance_time(st);   // physicalTime += dt (previous dt, DP/explicitLoop.cu:29)

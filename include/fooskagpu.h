@@ -308,6 +308,15 @@ int fg_checkpoint_read(fg_solver *s, const char *path);
  * export; |grad rho| from the most recent gradient pass). */
 int fg_field_dump(fg_solver *s, const char *path);
 
+/* Failure detection (the reference prints CUDA errors and continues).  fg_set_state rejects a
+ * state that is not finite, has alpha outside [0, 1] or a negative partial density
+ * (FG_ERR_NAN).  The RK kernels flag such a state when they produce it; the flag lives in mapped
+ * host memory, so fg_step checks it at entry without synchronising and returns FG_ERR_NAN from
+ * then on (the flag is seen once the flagged kernel has run: at most a few steps late).
+ * fg_check_state synchronises and reports it; *badStep = the step that produced it, or -1.
+ * fg_set_state / fg_checkpoint_read clear it. */
+int fg_check_state(fg_solver *s, int32_t *badStep);
+
 /* One explicitLoop iteration (DP/explicitLoop.cu:28-64): time advance, RK stages with the
  * adaptive dt at stage 0 every adaptDtItr steps, relaxation, conservation every adaptDtItr. */
 int fg_step(fg_solver *s, void *stream);
