@@ -61,6 +61,19 @@ def algorithmic_bytes(nf: float, fp64: bool):
 
 
 # ------------------------------------------------------------------ workload
+def mesh_setup_times(path: str, per) -> dict:
+    """Seconds to load the workload mesh (parse + connectivity + geometry + ordering) with the
+    host pre-processor and with the GPU one (identical arrays)."""
+    from fooskagpu_b200.api import Mesh
+    out = {}
+    for key, gpu in (("host_s", False), ("gpu_s", True)):
+        t0 = time.perf_counter()
+        m = Mesh.load_neu(path, scale=1.0, periodic=per, gpu=gpu)
+        out[key] = time.perf_counter() - t0
+        m.close()
+    return out
+
+
 def tgv_mesh(rank: int, world: int, dist):
     from fooskagpu_b200 import meshgen
     L = 2 * math.pi
@@ -158,7 +171,7 @@ def run_ours(args, rank, world, local_rank, dist):
     torch.cuda.set_device(local_rank)
     dev = local_rank
     path, per = tgv_mesh(rank, world, dist)
-    mesh = Mesh.load_neu(path, scale=1.0, periodic=per)
+    mesh = Mesh.load_neu(path, scale=1.0, periodic=per, gpu=True, device=dev)
     nE = mesh.n_elem
     info = mesh.info
     case = cases.tgv_case()
@@ -277,6 +290,9 @@ def run_ours(args, rank, world, local_rank, dist):
         kernels_fp64={k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]} for k, v in prof64.items()},
         clocks=cl,
     )
+    # ---------------- mesh pre-processing, host vs GPU (rank 0)
+    if rank == 0 and not args.no_mesh_timing:
+        out["mesh_preprocess"] = mesh_setup_times(path, per)
     # ---------------- two-phase workload with the Gibbs relaxation and the learned surrogate
     if not args.no_two_phase:
         out["two_phase"] = two_phase(args, torch, stream, dev)
@@ -488,6 +504,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="reference arm: skip timing the reference GPU build")
     ap.add_argument("--no-two-phase", action="store_true", help="skip the two-phase (surrogate) workload")
+    ap.add_argument("--no-mesh-timing", action="store_true", help="skip timing the host vs GPU mesh pre-processor")
     ap.add_argument("--n", type=int, default=None, help="cells per side of the TGV cube (default 128)")
     args = ap.parse_args()
     if args.n:

@@ -47,7 +47,8 @@ class FgCase(C.Structure):
 
 
 class FgMeshOpts(C.Structure):
-    _fields_ = [("scale", f64), ("periodic", f64 * 3), ("renumber", i32), ("reserved", i32 * 3)]
+    _fields_ = [("scale", f64), ("periodic", f64 * 3), ("renumber", i32), ("gpu", i32), ("device", i32),
+                ("reserved", i32 * 1)]
 
 
 class FgMeshInfo(C.Structure):

@@ -44,12 +44,16 @@ class Mesh:
         self.n_fcs = info.nFcs
 
     @classmethod
-    def load_neu(cls, path: str, scale: float = 1.0, periodic=(0.0, 0.0, 0.0), renumber: str = "morton") -> "Mesh":
+    def load_neu(cls, path: str, scale: float = 1.0, periodic=(0.0, 0.0, 0.0), renumber: str = "morton",
+                 gpu: bool = False, device: int = 0) -> "Mesh":
+        """gpu=True: face matching, face order, geometry and Morton order on the GPU (same arrays)."""
         o = FgMeshOpts()
         o.scale = scale
         for d in range(3):
             o.periodic[d] = periodic[d]
         o.renumber = _RENUM[renumber]
+        o.gpu = 1 if gpu else 0
+        o.device = device
         h = C.c_void_p()
         check(lib().fg_mesh_load_neu(path.encode(), C.byref(o), C.byref(h)))
         return cls(h)

@@ -46,7 +46,7 @@ def _run(cmd, cwd=None):
 
 def build_product(force: bool = False, verbose: bool = False, out: Path = None, defines=()) -> Path:
     cu = [CSRC / "fg_kernels.cu", CSRC / "fg_relax.cu", CSRC / "fg_solver.cu", CSRC / "fg_noalloc.cu",
-          CSRC / "fg_surrogate.cu"]
+          CSRC / "fg_surrogate.cu", CSRC / "fg_mesh_gpu.cu"]
     cpp = [CSRC / "fg_mesh.cpp"]
     hdr = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "fooskagpu.h"]
     lib_out = out or LIB
@@ -61,6 +61,9 @@ def build_product(force: bool = False, verbose: bool = False, out: Path = None, 
     for s in cu:
         o = objdir / (s.stem + ".o")
         cmd = [nvcc, *ARCH, "-lineinfo", *common, "-c", str(s), "-o", str(o)]
+        if s.name == "fg_mesh_gpu.cu":
+            # the mesh geometry must round exactly as the host path (no contracted multiply-adds)
+            cmd.insert(1, "--fmad=false")
         if s.name == "fg_kernels.cu":
             # the stage kernels' FP32 face math uses fast division / square root / FTZ (the FP32
             # path's tolerance allows ~2 ulp); FP64 code is unaffected by these flags

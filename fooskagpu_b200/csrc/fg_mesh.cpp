@@ -360,6 +360,14 @@ int finish_mesh(Mesh &m, const fg_mesh_opts &o, std::string &err) {
     }
     for (auto &kv : open) unmatched.push_back(kv.second);
     std::sort(unmatched.begin(), unmatched.end());
+    const int rc = match_periodic(m, o, unmatched, err);
+    if (rc != FG_OK) return rc;
+    return finish_order_geometry(m, o, err);
+}
+
+// Pair the open (unmatched, untagged) element faces periodically when the options ask for it;
+// any face still open is an error.  unmatched is sorted.
+int match_periodic(Mesh &m, const fg_mesh_opts &o, std::vector<int64_t> &unmatched, std::string &err) {
     m.nPeriodic = 0;
     // periodic matching (extension): pair untagged open faces whose centres differ by a box length
     const bool anyPer = o.periodic[0] > 0 || o.periodic[1] > 0 || o.periodic[2] > 0;
@@ -456,6 +464,12 @@ int finish_mesh(Mesh &m, const fg_mesh_opts &o, std::string &err) {
               " face " + std::to_string(ef % 6 + 1) + " (" + std::to_string(unmatched.size()) + " such faces)";
         return FG_ERR_MESH;
     }
+    return FG_OK;
+}
+
+// The reference face order, face and cell geometry and the device ordering (host path).
+int finish_order_geometry(Mesh &m, const fg_mesh_opts &o, std::string &err) {
+    const int nE = m.nElem;
     // reference face order: owner = first visited element (DP/buildLocalMesh.cu:263-313)
     m.fc2el.clear(); m.fc2elFc.clear(); m.boundCond.clear();
     m.fc2el.reserve((size_t)nE * 4); m.fc2elFc.reserve((size_t)nE * 4);

@@ -44,8 +44,13 @@ struct Mesh {
 // Parse a Gambit neutral file with the reference's grammar (DP/translator.cu:3-354).
 // Returns FG_OK or an error code with a message in err.
 int read_neu(const std::string &path, double scale, Mesh &m, std::string &err);
-// Match faces, build the reference face order and geometry, renumber.
+// Match faces, build the reference face order and geometry, renumber (host).
 int finish_mesh(Mesh &m, const fg_mesh_opts &o, std::string &err);
+// The same on the GPU (o.device); identical arrays.
+int finish_mesh_gpu(Mesh &m, const fg_mesh_opts &o, std::string &err);
+// parts shared by both paths
+int match_periodic(Mesh &m, const fg_mesh_opts &o, std::vector<int64_t> &unmatched, std::string &err);
+int finish_order_geometry(Mesh &m, const fg_mesh_opts &o, std::string &err);
 
 }  // namespace fg
 

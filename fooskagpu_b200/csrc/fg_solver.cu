@@ -825,7 +825,7 @@ int fg_mesh_load_neu(const char *path, const fg_mesh_opts *opts, fg_mesh **out) 
     std::string err;
     int rc = fg::read_neu(path, o.scale, m->m, err);
     if (rc != FG_OK) return set_err(rc, err);
-    rc = fg::finish_mesh(m->m, o, err);
+    rc = o.gpu ? fg::finish_mesh_gpu(m->m, o, err) : fg::finish_mesh(m->m, o, err);
     if (rc != FG_OK) return set_err(rc, err);
     *out = m.release();
     return FG_OK;

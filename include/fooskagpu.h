@@ -139,7 +139,10 @@ typedef struct fg_mesh_opts {
     double  scale;        /* coordinates are multiplied by this (reference: input.scale)   */
     double  periodic[3];  /* >0: box length of a periodic axis (extension; 0 = none)       */
     int32_t renumber;     /* enum fg_renumber for the device ordering                      */
-    int32_t reserved[3];
+    int32_t gpu;          /* 1: match faces, order them, compute the geometry and the Morton
+                             order on GPU `device` (same arrays as the host path; Morton or none) */
+    int32_t device;
+    int32_t reserved[1];
 } fg_mesh_opts;
 
 typedef struct fg_mesh_info {
