@@ -79,17 +79,18 @@ struct Fields {
     double *signal;     // [n]
     double *blockMin;   // [nBlocks]
     double *dt;         // device scalar
-    int32_t *bad;       // set to the step counter + 1 when an updated state is not finite or has a
-                        // negative partial density (sticky until cleared; mapped host memory)
+    int32_t *bad;       // set to the step counter + 1 when an updated state is not finite or its
+                        // mixture density is not positive (sticky until cleared; mapped host memory)
     int32_t step;       // the step counter the kernels record
 };
 
-// the updated conserved state of a cell is usable: finite, 0 <= alpha <= 1, partial densities >= 0
+// the updated conserved state of a cell is usable: finite with a positive mixture density (alpha
+// itself may leave [0, 1] by rounding: cons2prim clamps it, DP/cons2prim.h:6)
 __device__ __forceinline__ bool state_ok(const double *u) {
     double s = 0;
 #pragma unroll
     for (int v = 0; v < NV; v++) s += u[v];
-    return isfinite(s) && u[0] >= 0.0 && u[0] <= 1.0 && u[1] >= 0.0 && u[2] >= 0.0;
+    return isfinite(s) && u[1] + u[2] > 0.0;
 }
 
 enum FluxMode { FLUX_FUSED = 0, FLUX_RHS = 1 };

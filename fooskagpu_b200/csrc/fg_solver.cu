@@ -80,7 +80,7 @@ struct fg_solver {
         return FG_OK;
     }
     int bad_state_error() const {
-        return set_err(FG_ERR_NAN, "the state became non-finite or got a negative partial density in step " +
+        return set_err(FG_ERR_NAN, "the state became non-finite or its density non-positive in step " +
                                        std::to_string(*hBad - 1) + " (reset it with fg_set_state / fg_checkpoint_read)");
     }
     int device = 0;
@@ -163,10 +163,12 @@ struct fg_solver {
 
 namespace fg {
 
+// an uploaded state: finite, alpha in [0, 1] (within 1e-9), partial densities not negative
 inline bool state_ok_host(const double *u) {
     double sum = 0;
     for (int v = 0; v < NV; v++) sum += u[v];
-    return std::isfinite(sum) && u[0] >= 0.0 && u[0] <= 1.0 && u[1] >= 0.0 && u[2] >= 0.0;
+    return std::isfinite(sum) && u[0] >= -1e-9 && u[0] <= 1.0 + 1e-9 && u[1] >= 0.0 && u[2] >= 0.0 &&
+           u[1] + u[2] > 0.0;
 }
 
 __global__ void k_advance_time(const double *dt, double *t) { *t += *dt; }

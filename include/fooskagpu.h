@@ -313,7 +313,9 @@ int fg_field_dump(fg_solver *s, const char *path);
 
 /* Failure detection (the reference prints CUDA errors and continues).  fg_set_state rejects a
  * state that is not finite, has alpha outside [0, 1] or a negative partial density
- * (FG_ERR_NAN).  The RK kernels flag such a state when they produce it; the flag lives in mapped
+ * (FG_ERR_NAN).  The RK kernels flag a state they produce that is not finite or has a
+ * non-positive mixture density (alpha may leave [0, 1] by rounding; cons2prim clamps it, as in
+ * the reference); the flag lives in mapped
  * host memory, so fg_step checks it at entry without synchronising and returns FG_ERR_NAN from
  * then on (the flag is seen once the flagged kernel has run: at most a few steps late).
  * fg_check_state synchronises and reports it; *badStep = the step that produced it, or -1.
