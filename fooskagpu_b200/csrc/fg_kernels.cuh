@@ -141,6 +141,9 @@ struct RelaxOrder {
     int32_t *blockOff;   // [relax_order_blocks(n)]
     int32_t *order;      // [n]
     int32_t *total;      // [1] chemical cells
+    float4 *pred;        // [n] surrogate prediction of the chemical cell order[i]
+    int32_t *hullOk;     // [n] its input is inside the training hull
+    int32_t *tcErr;      // [1] a tensor-core completion wait timed out
 };
 int relax_order_blocks(int n);
 // returns the number of kernels launched

@@ -11,7 +11,7 @@
 // reference's residuals; it is accepted when every relative residual is within `relTol`,
 // otherwise (and outside the hull) the cell takes the reference Newton unchanged.
 #include "fg_kernels.cuh"
-#include "fg_surrogate.cuh"
+#include "fg_sg_tc.cuh"
 
 namespace fg {
 
@@ -437,10 +437,32 @@ __global__ void k_relax_order(int n, const uint8_t *isChem, const int32_t *block
 // carries none of their code (and none of their registers).  kOrd: thread i relaxes cell
 // order[i], chemical when i < *nChem (k_relax_order); otherwise thread i relaxes cell i and
 // decides the branch itself.
+// surrogate input of the relaxation: chemical cell order[i], i < *nChem
+struct InRelax {
+    const double *U;
+    int n;
+    const int32_t *order;
+    const int32_t *nChem;
+    RelaxParams R;
+    __device__ int count() const { return *nChem; }
+    __device__ void features(int i, const SurrogateNorm &N, float (&z)[3]) const {
+        const int c = order[i];
+        double u[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
+        double rm, re, ag;
+        chem_mixture(R, u, &rm, &re, &ag);
+        const float f[3] = {(float)rm, (float)(re / rm), (float)(ag / rm)};
+#pragma unroll
+        for (int k = 0; k < 3; k++) z[k] = (f[k] - N.xMean[k]) / N.xStd[k];
+    }
+};
+
 template <typename T, bool kSG, bool kLog, bool kOrd>
 __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R,
                                                int32_t *counters, const SurrogateDev S, const RelaxLog Lg,
-                                               const int32_t *order, const int32_t *nChem) {
+                                               const int32_t *order, const int32_t *nChem, const float4 *pred,
+                                               const int32_t *hullOk) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool act = i < n;
     const int c = (kOrd && act) ? order[i] : i;
@@ -448,7 +470,6 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
     const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
     double u[NV];
     double rm = 0, re = 0, ag = 0;
-    float z[3] = {0.f, 0.f, 0.f};
     bool want = false;
     if (act) {
 #pragma unroll
@@ -456,25 +477,18 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
         if (R.chemFlag == 1) chem = kOrd ? (i < *nChem) : needs_chem(R, h, u);
         if (chem && (kSG || kLog)) {
             chem_mixture(R, u, &rm, &re, &ag);
-            if (kSG) {
-                const float f[3] = {(float)rm, (float)(re / rm), (float)(ag / rm)};
-#pragma unroll
-                for (int k = 0; k < 3; k++) z[k] = (f[k] - S.norm.xMean[k]) / S.norm.xStd[k];
-                want = sg_in_hull(S.norm, z);
-            }
+            // the network's prediction for this cell (k_sg_tc over the chemical cells) if its
+            // input is inside the training hull
+            if (kSG) want = hullOk[i] != 0;
         }
-    }
-    // the network runs once per warp that has a candidate cell (all 32 lanes take part)
-    float pred[4] = {0.f, 0.f, 0.f, 0.f};
-    if (kSG && __any_sync(0xffffffffu, want)) {
-        float o[4];
-        sg_warp_forward(S, z, o);
-#pragma unroll
-        for (int k = 0; k < 4; k++) pred[k] = S.norm.yMean[k] + S.norm.yStd[k] * o[k];
     }
     if (act) {
         int pits = 0;
-        if (kSG && want) used = chem_polish(R, h, u, pred, rm, re, S.relTol, S.polishIters, &pits);
+        if (kSG && want) {
+            const float4 p4 = pred[i];
+            const float pr[4] = {p4.x, p4.y, p4.z, p4.w};
+            used = chem_polish(R, h, u, pr, rm, re, S.relTol, S.polishIters, &pits);
+        }
         if (!used) {
             ab = chem ? chem_cell(R, h, u, &its) : therm_cell(R, h, u, &its);
             if (kLog && chem && !ab) {
@@ -530,30 +544,44 @@ int relax_order_blocks(int n) { return (n + kOrdThreads - 1) / kOrdThreads; }
 
 template <typename T, bool kOrd>
 static void launch_relax_k(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
-                           const SurrogateDev &S, const RelaxLog &L, const int32_t *order, const int32_t *nChem,
-                           cudaStream_t s) {
+                           const SurrogateDev &S, const RelaxLog &L, const RelaxOrder *O, cudaStream_t s) {
     const int nb = (n + 127) / 128;
     const bool lg = L.count != nullptr;
-    if (S.enabled && lg) k_relax<T, true, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem);
-    else if (S.enabled) k_relax<T, true, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem);
-    else if (lg) k_relax<T, false, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem);
-    else k_relax<T, false, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem);
+    const int32_t *order = O ? O->order : nullptr, *nChem = O ? O->total : nullptr;
+    const float4 *pred = O ? O->pred : nullptr;
+    const int32_t *hull = O ? O->hullOk : nullptr;
+    if (kOrd && S.enabled && lg)
+        k_relax<T, true, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem, pred, hull);
+    else if (kOrd && S.enabled)
+        k_relax<T, true, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem, pred, hull);
+    else if (lg)
+        k_relax<T, false, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem, pred, hull);
+    else
+        k_relax<T, false, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem, pred, hull);
 }
 
 template <typename T>
 int launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
                  const SurrogateDev &S, const RelaxLog &L, const RelaxOrder &O, cudaStream_t s) {
     if (R.chemFlag != 1) {
-        // every cell is thermal: no ordering needed
-        launch_relax_k<T, false>(n, U, W, D, R, counters, S, L, nullptr, nullptr, s);
+        // every cell is thermal: no ordering needed (and no surrogate)
+        launch_relax_k<T, false>(n, U, W, D, R, counters, SurrogateDev{}, L, nullptr, s);
         return 1;
     }
     const int nb = relax_order_blocks(n);
     k_relax_partition<<<nb, kOrdThreads, 0, s>>>(n, U, R, O.isChem, O.blockCnt);
     k_relax_scan<<<1, 1024, 0, s>>>(O.blockCnt, nb, O.blockOff, O.total);
     k_relax_order<<<nb, kOrdThreads, 0, s>>>(n, O.isChem, O.blockOff, O.total, O.order);
-    launch_relax_k<T, true>(n, U, W, D, R, counters, S, L, O.order, O.total, s);
-    return 4;
+    int k = 4;
+    if (S.enabled) {
+        // the network on the tensor cores for the chemical cells (order[0 .. nChem)), tiles of 128
+        const int tiles = (n + TC_M - 1) / TC_M;
+        k_sg_tc<InRelax><<<std::min(tiles, 148 * 4), 128, TC_SMEM, s>>>(S, S.pack, InRelax{U, n, O.order, O.total, R},
+                                                                        O.pred, O.hullOk, O.tcErr);
+        k++;
+    }
+    launch_relax_k<T, true>(n, U, W, D, R, counters, S, L, &O, s);
+    return k;
 }
 
 template int launch_relax<float>(int, double *, float *, const PhysD &, const RelaxParams &, int32_t *,

@@ -216,6 +216,7 @@ struct SolverT : public fg_solver {
     DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dBlockMin, dScal, dCnt, dCons, dStage;
     DevBuf dFIdx, dFGeo, dSlotFace, dClosure, dFB;
     DevBuf dOrdFlag, dOrdCnt, dOrdOff, dOrder, dOrdTotal;   // relaxation cell ordering
+    DevBuf dPred, dHullOk, dTcErr;                          // surrogate predictions
     int cur = 0;
     DevMesh<T> dm{};
     PhysT<T> P{};
@@ -495,6 +496,10 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dOrdOff.alloc((size_t)relax_order_blocks(n) * sizeof(int32_t)));
         FG_CUDA_TRY(dOrder.alloc((size_t)n * sizeof(int32_t)));
         FG_CUDA_TRY(dOrdTotal.alloc(sizeof(int32_t)));
+        FG_CUDA_TRY(dPred.alloc((size_t)n * sizeof(float4)));
+        FG_CUDA_TRY(dHullOk.alloc((size_t)n * sizeof(int32_t)));
+        FG_CUDA_TRY(dTcErr.alloc(sizeof(int32_t)));
+        FG_CUDA_TRY(cudaMemset(dTcErr.p, 0, sizeof(int32_t)));
         FG_CUDA_TRY(cudaMemset(dU.p, 0, u));
         FG_CUDA_TRY(cudaMemset(dU0.p, 0, u));
         FG_CUDA_TRY(cudaMemset(dRHS.p, 0, u));
@@ -506,7 +511,8 @@ struct SolverT : public fg_solver {
         bytes = 0;
         for (DevBuf *b : {&dNbr, &dFlags, &dGeo, &dVol, &dVolP, &dNew2Old, &dU, &dU0, &dRHS, &dStage, &dW[0], &dW[1], &dG,
                           &dSig, &dBlockMin, &dScal, &dCnt, &dHaloStart, &dHaloIds, &dSlotLocal, &dFIdx, &dFGeo,
-                          &dSlotFace, &dClosure, &dFB, &dOrdFlag, &dOrdCnt, &dOrdOff, &dOrder, &dOrdTotal})
+                          &dSlotFace, &dClosure, &dFB, &dOrdFlag, &dOrdCnt, &dOrdOff, &dOrder, &dOrdTotal,
+                          &dPred, &dHullOk, &dTcErr})
             bytes += b->bytes;
         dm.n = n;
         dm.nSlots = nSlots;
@@ -643,7 +649,7 @@ struct SolverT : public fg_solver {
         }
         RelaxLog L{logX.as<float>(), logY.as<float>(), logCap > 0 ? logCnt.as<unsigned long long>() : nullptr, logCap};
         const RelaxOrder O{dOrdFlag.as<uint8_t>(), dOrdCnt.as<int32_t>(), dOrdOff.as<int32_t>(), dOrder.as<int32_t>(),
-                           dOrdTotal.as<int32_t>()};
+                           dOrdTotal.as<int32_t>(), dPred.as<float4>(), dHullOk.as<int32_t>(), dTcErr.as<int32_t>()};
         prof_begin(FG_K_RELAX, s);
         const int k = launch_relax<T>(n, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), S, L, O, s);
         prof_end(s);

@@ -8,7 +8,7 @@
 // parameters are FP32 with Adam.  Every reduction over samples (weight gradients, loss) sums
 // fixed chunks in a fixed order, so training is deterministic for a given seed.
 #include "../../include/fooskagpu.h"
-#include "fg_surrogate.cuh"
+#include "fg_sg_tc.cuh"
 
 #include <cuda_runtime.h>
 
@@ -157,23 +157,16 @@ __global__ void k_adam(float *P, const float *G, float *M, float *V, int n, floa
     P[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
 }
 
-// batch prediction through the tensor-core forward: raw inputs -> raw outputs, hull flag
-__global__ void k_sg_predict(const SurrogateDev S, const float *X, int n, float *Y, int32_t *inHull) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool act = i < n;
-    float z[3] = {0.f, 0.f, 0.f};
-    if (act) {
+// batch prediction input: raw samples X[n][3]
+struct InPredict {
+    const float *X;
+    int n;
+    __device__ int count() const { return n; }
+    __device__ void features(int i, const SurrogateNorm &N, float (&z)[3]) const {
 #pragma unroll
-        for (int k = 0; k < 3; k++) z[k] = (X[(size_t)i * 3 + k] - S.norm.xMean[k]) / S.norm.xStd[k];
+        for (int k = 0; k < 3; k++) z[k] = (X[(size_t)i * 3 + k] - N.xMean[k]) / N.xStd[k];
     }
-    float o[4];
-    sg_warp_forward(S, z, o);
-    if (act) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) Y[(size_t)i * 4 + k] = S.norm.yMean[k] + S.norm.yStd[k] * o[k];
-        if (inHull) inHull[i] = sg_in_hull(S.norm, z) ? 1 : 0;
-    }
-}
+};
 
 // ---------------------------------------------------------------- host helpers
 uint16_t bf16_rne(float f) {
@@ -185,19 +178,14 @@ uint16_t bf16_rne(float f) {
     return (uint16_t)(u >> 16);
 }
 
-// B fragments of one layer W[K][N] (row-major, in x out) for mma.m16n8k16 (see fg_surrogate.cuh)
-void pack_layer(const float *W, int K, int N, int KT, int NT, uint32_t *out) {
-    auto w = [&](int k, int n) -> uint32_t { return (k < K && n < N) ? bf16_rne(W[k * N + n]) : 0u; };
-    for (int kk = 0; kk < KT; kk++)
-        for (int j = 0; j < NT; j++)
-            for (int lane = 0; lane < 32; lane++) {
-                const int g = lane >> 2, t = lane & 3;
-                const int n = 8 * j + g;
-                const int k0 = 16 * kk + 2 * t;
-                uint32_t *o = out + ((size_t)(kk * NT + j) * 32 + lane) * 2;
-                o[0] = w(k0, n) | (w(k0 + 1, n) << 16);
-                o[1] = w(k0 + 8, n) | (w(k0 + 9, n) << 16);
-            }
+// one layer W[K][N] (row-major, in x out) as the B operand of the tensor-core layer: N rows of
+// K (K-major), K padded to 16 * kSlabs and N to nPad with zeros, in the canonical layout
+void pack_layer_tc(const float *W, int K, int N, int kSlabs, int nPad, unsigned char *out) {
+    for (int n = 0; n < nPad; n++)
+        for (int k = 0; k < 16 * kSlabs; k++) {
+            const uint16_t v = (k < K && n < N) ? bf16_rne(W[k * N + n]) : (uint16_t)0;
+            std::memcpy(out + tc_smem_off_host(n, k, nPad), &v, 2);
+        }
 }
 
 bool invert3(const double *a, double *inv) {
@@ -249,12 +237,12 @@ struct fg_surrogate {
     int repack() {
         std::vector<float> p(SG_NPARAM);
         SG_TRY(cudaMemcpy(p.data(), P.p, SG_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
-        std::vector<uint32_t> pk(SG_PK_TOTAL, 0u);
-        pack_layer(p.data() + SG_OFF_W1, SG_IN, SG_H, 1, 8, pk.data() + SG_PK_L1);
-        pack_layer(p.data() + SG_OFF_W2, SG_H, SG_H, 4, 8, pk.data() + SG_PK_L2);
-        pack_layer(p.data() + SG_OFF_W3, SG_H, SG_H, 4, 8, pk.data() + SG_PK_L3);
-        pack_layer(p.data() + SG_OFF_W4, SG_H, SG_OUT, 4, 1, pk.data() + SG_PK_L4);
-        SG_TRY(cudaMemcpy(pack.p, pk.data(), SG_PK_TOTAL * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        std::vector<unsigned char> pk(TC_WBYTES, 0);
+        pack_layer_tc(p.data() + SG_OFF_W1, SG_IN, SG_H, 1, 64, pk.data() + TC_W1);
+        pack_layer_tc(p.data() + SG_OFF_W2, SG_H, SG_H, 4, 64, pk.data() + TC_W2);
+        pack_layer_tc(p.data() + SG_OFF_W3, SG_H, SG_H, 4, 64, pk.data() + TC_W3);
+        pack_layer_tc(p.data() + SG_OFF_W4, SG_H, SG_OUT, 4, 16, pk.data() + TC_W4);
+        SG_TRY(cudaMemcpy(pack.p, pk.data(), TC_WBYTES, cudaMemcpyHostToDevice));
         return FG_OK;
     }
 
@@ -310,7 +298,7 @@ namespace fg {
 // device view of a surrogate for the relaxation kernel
 int surrogate_view(const fg_surrogate *g, SurrogateDev *out) {
     if (!g || !g->hasNorm) return fg::set_error(FG_ERR_ARG, "surrogate has no training data statistics");
-    out->pack = g->pack.as<uint32_t>();
+    out->pack = g->pack.as<unsigned char>();
     out->params = g->P.as<float>();
     out->norm = g->norm;
     out->enabled = 1;
@@ -331,7 +319,7 @@ int fg_surrogate_create(int32_t device, uint64_t seed, fg_surrogate **out) {
     auto fail = [&](int code) { delete g; return code; };
     if (cudaSuccess != g->P.alloc(SG_NPARAM * sizeof(float)) || cudaSuccess != g->G.alloc(SG_NPARAM * sizeof(float)) ||
         cudaSuccess != g->M.alloc(SG_NPARAM * sizeof(float)) || cudaSuccess != g->V.alloc(SG_NPARAM * sizeof(float)) ||
-        cudaSuccess != g->pack.alloc(SG_PK_TOTAL * sizeof(uint32_t)))
+        cudaSuccess != g->pack.alloc(TC_WBYTES))
         return fail(fg::set_error(FG_ERR_NOMEM, "fg_surrogate_create: device allocation failed"));
     // He-style initialisation: W ~ N(0, 2 / fan_in), b = 0 (seeded, reproducible)
     std::vector<float> p(SG_NPARAM, 0.f);
@@ -525,13 +513,20 @@ int fg_surrogate_predict(fg_surrogate *g, const float *X, int32_t n, float *Y, i
     SurrogateDev S{};
     int rc = surrogate_view(g, &S);
     if (rc != FG_OK) return rc;
-    Buf dx, dy, dh;
+    Buf dx, dy, dh, de;
     SG_TRY(dx.alloc((size_t)n * 3 * sizeof(float)));
     SG_TRY(dy.alloc((size_t)n * 4 * sizeof(float)));
     SG_TRY(dh.alloc((size_t)n * sizeof(int32_t)));
+    SG_TRY(de.alloc(sizeof(int32_t)));
+    SG_TRY(cudaMemset(de.p, 0, sizeof(int32_t)));
     SG_TRY(cudaMemcpy(dx.p, X, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice));
-    k_sg_predict<<<(n + 127) / 128, 128>>>(S, dx.as<float>(), n, dy.as<float>(), dh.as<int32_t>());
+    const int tiles = (n + TC_M - 1) / TC_M;
+    k_sg_tc<InPredict><<<std::min(tiles, 148 * 4), 128, TC_SMEM>>>(S, S.pack, InPredict{dx.as<float>(), n},
+                                                                   dy.as<float4>(), dh.as<int32_t>(), de.as<int32_t>());
     SG_TRY(cudaGetLastError());
+    int32_t terr = 0;
+    SG_TRY(cudaMemcpy(&terr, de.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (terr) return fg::set_error(FG_ERR_CUDA, "fg_surrogate_predict: tensor-core completion wait timed out");
     SG_TRY(cudaMemcpy(Y, dy.p, (size_t)n * 4 * sizeof(float), cudaMemcpyDeviceToHost));
     if (inHull) SG_TRY(cudaMemcpy(inHull, dh.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
     return FG_OK;
