@@ -338,7 +338,7 @@ __device__ __forceinline__ void cell_grad_t(const PhysT<T> &P, const T *w, const
 //   var 0: -alpha_c s u,  vars 6/7: +alpha_c pL_c s u, +(1-alpha_c) pG_c s u,
 //   momentum: -pC_c s A n summed = pC_c * (sum of outward n A)  (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
 template <typename T>
-__global__ void __launch_bounds__(128, MinBlocks<T>::face) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
+__global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
                                               T *__restrict__ FB, const PhysT<T> P, int wantSignal) {
     const int fi = blockIdx.x * blockDim.x + threadIdx.x;
     if (fi >= m.nF) return;
@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::face) k_face(const DevMesh<
 
 // ------------------------------------------------------------------ owner-side gather + RK
 template <typename T>
-__global__ void __launch_bounds__(256, MinBlocks<T>::gather) k_gather(const DevMesh<T> m, Fields<T> f, const PhysD D, int mode,
+__global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gather(const DevMesh<T> m, Fields<T> f, const PhysD D, int mode,
                                                 int wantSignal, StageCoef sc) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;
@@ -629,7 +629,7 @@ __global__ void k_copy(size_t cnt, const double *__restrict__ a, double *b) {
 }
 
 // ------------------------------------------------------------------ launchers
-constexpr int kGatherThreads = 256;
+constexpr int kGatherThreads = FG_GATHER_THREADS;
 int flux_blocks(int n) { return (n + kGatherThreads - 1) / kGatherThreads; }
 int cons_blocks(int n) { return (n + kConsThreads - 1) / kConsThreads; }
 
@@ -660,7 +660,7 @@ void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cud
 }
 template <typename T>
 void launch_face(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, int wantSignal, cudaStream_t s) {
-    k_face<T><<<(m.nF + 127) / 128, 128, 0, s>>>(m, f.Win, f.G, f.FB, P, wantSignal);
+    k_face<T><<<(m.nF + FG_FACE_THREADS - 1) / FG_FACE_THREADS, FG_FACE_THREADS, 0, s>>>(m, f.Win, f.G, f.FB, P, wantSignal);
 }
 template <typename T>
 void launch_gather(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, int mode, int wantSignal,

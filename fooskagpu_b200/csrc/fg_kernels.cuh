@@ -62,7 +62,15 @@ constexpr int FREC = 12;
 // kernels are latency-bound gathers: capping registers at 85 / 85 / 51 per thread (6, 6, 5
 // blocks) raises the warps in flight and measured 2-9 % faster on the 128^3 hex workload.  The
 // FP64 kernels need their registers (capping them spills): 0 leaves the choice to the compiler.
-template <typename T> struct MinBlocks { static constexpr int grad = 6, face = 6, gather = 5; };
+#ifndef FG_FACE_THREADS
+#define FG_FACE_THREADS 64
+#endif
+#ifndef FG_GATHER_THREADS
+#define FG_GATHER_THREADS 128
+#endif
+template <typename T> struct MinBlocks {
+    static constexpr int grad = 6, face = 6 * 128 / FG_FACE_THREADS, gather = 5 * 256 / FG_GATHER_THREADS;
+};
 template <> struct MinBlocks<double> { static constexpr int grad = 0, face = 0, gather = 0; };
 template <typename T> struct StageCells { static constexpr int value = FG_STAGE_CELLS_F; };
 template <> struct StageCells<double> { static constexpr int value = FG_STAGE_CELLS_D; };
