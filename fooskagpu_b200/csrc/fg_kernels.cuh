@@ -59,8 +59,8 @@ constexpr int FREC = 12;
 #define FG_STAGE_GEOMETRY 0
 #endif
 // Minimum resident blocks per SM asked of the compiler (its register budget).  The FP32 stage
-// kernels are latency-bound gathers: capping registers at 85 / 85 / 51 per thread (6, 6, 5
-// blocks) raises the warps in flight and measured 2-9 % faster on the 128^3 hex workload.  The
+// kernels are latency-bound gathers: capping registers at 85 / 85 / 51 per thread (gradient,
+// face, gather) raises the warps in flight and measured 2-9 % faster on the 128^3 hex workload.  The
 // FP64 kernels need their registers (capping them spills): 0 leaves the choice to the compiler.
 #ifndef FG_FACE_THREADS
 #define FG_FACE_THREADS 64
