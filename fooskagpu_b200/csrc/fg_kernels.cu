@@ -643,12 +643,17 @@ template <typename T>
 static size_t grad_smem(const DevMesh<T> &m) {
     return rec_area<T>(m, Stage<T>::WS) + geo_smem(m);
 }
+// raise (never lower) a kernel's dynamic shared-memory limit on the current device: solvers of
+// different meshes launch the same kernels with different amounts
+static int raise_smem(const void *fn, size_t bytes) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, fn) != cudaSuccess) return 1;
+    if ((size_t)a.maxDynamicSharedSizeBytes >= bytes) return 0;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess;
+}
 template <typename T>
 int stage_kernels_setup(const DevMesh<T> &m) {
-    if (cudaFuncSetAttribute(k_grad<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem(m)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_grad<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grad_smem(m)) != cudaSuccess)
-        return 1;
-    return 0;
+    return raise_smem((const void *)k_grad<T, 0>, grad_smem(m)) | raise_smem((const void *)k_grad<T, 1>, grad_smem(m));
 }
 template <typename T>
 void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cudaStream_t s) {
