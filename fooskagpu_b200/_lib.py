@@ -74,6 +74,20 @@ class FgRelaxStats(C.Structure):
                 ("nFallback", i32)]
 
 
+class FgPartitionInfo(C.Structure):
+    _fields_ = [("nParts", i32), ("part", i32), ("nOwned", i32), ("nGhost", i32), ("nSend", i32), ("nRecv", i32)]
+
+
+FG_HALO_W, FG_HALO_G = 0, 1
+FG_REDUCE_MIN, FG_REDUCE_SUM = 0, 1
+HALO_EXCHANGE_FN = C.CFUNCTYPE(C.c_int, VP, i32, i64, VP)
+HALO_ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, VP, i32, PD)
+
+
+class FgHaloOps(C.Structure):
+    _fields_ = [("ctx", VP), ("exchange", HALO_EXCHANGE_FN), ("allreduce", HALO_ALLREDUCE_FN)]
+
+
 # name -> (restype, argtypes); every symbol here is declared in include/fooskagpu.h
 SIGNATURES = {
     "fg_last_error": (C.c_char_p, []),
@@ -83,6 +97,11 @@ SIGNATURES = {
     "fg_mesh_view_get": (C.c_int, [VP, C.POINTER(FgMeshView)]),
     "fg_mesh_permutation": (C.c_int, [VP, PI, i32]),
     "fg_mesh_free": (None, [VP]),
+    "fg_mesh_partition": (C.c_int, [VP, i32, i32, C.POINTER(VP)]),
+    "fg_mesh_partition_info": (C.c_int, [VP, C.POINTER(FgPartitionInfo)]),
+    "fg_mesh_partition_maps": (C.c_int, [VP, PI, PI, PI, PI, PI]),
+    "fg_halo_buffer_bytes": (C.c_int, [VP, C.POINTER(i64), C.POINTER(i64)]),
+    "fg_solver_set_halo": (C.c_int, [VP, C.POINTER(FgHaloOps), VP, VP]),
     "fg_solver_create": (C.c_int, [VP, C.POINTER(FgCase), i32, i32, C.POINTER(VP)]),
     "fg_solver_destroy": (C.c_int, [VP]),
     "fg_solver_memory": (C.c_int, [VP, C.POINTER(C.c_uint64)]),

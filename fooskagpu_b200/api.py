@@ -42,6 +42,10 @@ class Mesh:
         self.info = {k: getattr(info, k) for k, _ in FgMeshInfo._fields_}
         self.n_elem = info.nElem
         self.n_fcs = info.nFcs
+        pi = L.FgPartitionInfo()
+        check(lib().fg_mesh_partition_info(self._h, C.byref(pi)))
+        self.part_info = {k: getattr(pi, k) for k, _ in L.FgPartitionInfo._fields_}
+        self.n_owned = pi.nOwned   # cells with a state (all of them unless the mesh is a part)
 
     @classmethod
     def load_neu(cls, path: str, scale: float = 1.0, periodic=(0.0, 0.0, 0.0), renumber: str = "morton",
@@ -81,6 +85,27 @@ class Mesh:
             "nbShift": g(v.nbShift, 3 * nF).reshape(nF, 3),
         }
 
+    def partition(self, n_parts: int, part: int) -> "Mesh":
+        """Part `part` of `n_parts` (contiguous ranges of the Morton device order): own cells first,
+        then one layer of ghost cells; the returned mesh is independent of this one."""
+        h = C.c_void_p()
+        check(lib().fg_mesh_partition(self._h, int(n_parts), int(part), C.byref(h)))
+        return Mesh(h)
+
+    def partition_maps(self) -> dict:
+        """cell_global (.neu index in the whole mesh of each cell), send/recv lists per part."""
+        pi = self.part_info
+        P = pi["nParts"]
+        out = {"cell_global": np.empty(self.n_elem, np.int32), "send_start": np.empty(P + 1, np.int32),
+               "send_cells": np.empty(max(pi["nSend"], 1), np.int32), "recv_start": np.empty(P + 1, np.int32),
+               "recv_cells": np.empty(max(pi["nRecv"], 1), np.int32)}
+        check(lib().fg_mesh_partition_maps(self._h, *(out[k].ctypes.data_as(L.PI) for k in
+                                                      ("cell_global", "send_start", "send_cells", "recv_start",
+                                                       "recv_cells"))))
+        out["send_cells"] = out["send_cells"][:pi["nSend"]]
+        out["recv_cells"] = out["recv_cells"][:pi["nRecv"]]
+        return out
+
     def permutation(self) -> np.ndarray:
         p = np.empty(self.n_elem, dtype=np.int32)
         check(lib().fg_mesh_permutation(self._h, p.ctypes.data_as(L.PI), self.n_elem))
@@ -108,7 +133,8 @@ class Solver:
         h = C.c_void_p()
         check(lib().fg_solver_create(mesh._h, C.byref(case), _PREC[precision], device, C.byref(h)))
         self._h = h
-        self.n = mesh.n_elem
+        self.n = mesh.n_owned     # state rows: the own cells of a part mesh
+        self._halo = None
 
     # -- state
     def set_state(self, U: np.ndarray, stream: Optional[int] = None) -> None:
@@ -120,6 +146,38 @@ class Solver:
             out = np.empty((self.n, 10), dtype=np.float64)
         check(lib().fg_get_state(self._h, _dptr(out), stream))
         return out
+
+    def halo_buffer_bytes(self):
+        sb, rb = L.i64(), L.i64()
+        check(lib().fg_halo_buffer_bytes(self._h, C.byref(sb), C.byref(rb)))
+        return sb.value, rb.value
+
+    def set_halo(self, exchange, allreduce, send_ptr: int, recv_ptr: int) -> None:
+        """Transport of a partitioned run: exchange(field, record_bytes, stream) moves the send
+        buffer's records to the other parts and fills the receive buffer; allreduce(op, value)
+        returns the combined value.  Both return normally on success (an exception is reported
+        to the solver as a failed exchange)."""
+        def _ex(ctx, field, rb, stream):
+            try:
+                exchange(int(field), int(rb), stream)
+                return 0
+            except Exception:
+                import traceback
+                traceback.print_exc()
+                return 1
+
+        def _ar(ctx, op, value):
+            try:
+                value[0] = float(allreduce(int(op), float(value[0])))
+                return 0
+            except Exception:
+                import traceback
+                traceback.print_exc()
+                return 1
+
+        ops = L.FgHaloOps(None, L.HALO_EXCHANGE_FN(_ex), L.HALO_ALLREDUCE_FN(_ar))
+        check(lib().fg_solver_set_halo(self._h, C.byref(ops), send_ptr, recv_ptr))
+        self._halo = ops   # the callbacks must outlive the solver's use of them
 
     # -- stage functions
     def compute_rhs(self, want_signal: bool = False, stream=None) -> None:

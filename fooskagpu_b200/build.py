@@ -47,7 +47,7 @@ def _run(cmd, cwd=None):
 def build_product(force: bool = False, verbose: bool = False, out: Path = None, defines=()) -> Path:
     cu = [CSRC / "fg_kernels.cu", CSRC / "fg_relax.cu", CSRC / "fg_solver.cu", CSRC / "fg_noalloc.cu",
           CSRC / "fg_surrogate.cu", CSRC / "fg_mesh_gpu.cu"]
-    cpp = [CSRC / "fg_mesh.cpp"]
+    cpp = [CSRC / "fg_mesh.cpp", CSRC / "fg_partition.cpp"]
     hdr = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "fooskagpu.h"]
     lib_out = out or LIB
     if not force and not _stale(lib_out, cu + cpp + hdr):

@@ -209,7 +209,8 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     const int b = blockIdx.x;
     const int B = m.blockCells;
     const int lo = b * B;
-    const int nOwn = min(B, m.n - lo);
+    const int nOwn = min(B, m.nU - lo);      // cells whose gradients this block computes
+    const int nBlockRecs = min(B, m.n - lo);  // cells of the block range with records (ghosts of a part too)
     const int nRec = B + (m.haloStart[b + 1] - m.haloStart[b]);
     const int SS = slot_stride(m.nSlots);
     T *rec = reinterpret_cast<T *>(smem_raw);                       // nRecMax * WS
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
         const V *Wv = reinterpret_cast<const V *>(W);
         for (int i = threadIdx.x; i < nRec * WV; i += blockDim.x) {
             const int r = i / WV, q = i - (i / WV) * WV;
-            const int src = staged_source(m, b, r, lo, nOwn);
+            const int src = staged_source(m, b, r, lo, nBlockRecs);
             if (src < 0) continue;
             const V x = __ldg(Wv + (size_t)src * WV + q);
             const T *xs = reinterpret_cast<const T *>(&x);
@@ -433,7 +434,7 @@ template <typename T>
 __global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gather(const DevMesh<T> m, Fields<T> f, const PhysD D, int mode,
                                                 int wantSignal, StageCoef sc) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n = m.n;
+    const int n = m.nU;   // state rows (U, U0, RHS stride)
     double cfl = 1e12;
     if (c < n) {
         const int fl = m.flags[c];
@@ -461,8 +462,8 @@ __global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gat
         acc[6] += a * pl * su;
         acc[7] += (1.0 - a) * pg * su;
         acc[3] += pc * (double)m.closure[c];
-        acc[4] += pc * (double)m.closure[(size_t)n + c];
-        acc[5] += pc * (double)m.closure[2 * (size_t)n + c];
+        acc[4] += pc * (double)m.closure[(size_t)m.n + c];
+        acc[5] += pc * (double)m.closure[2 * (size_t)m.n + c];
         const double vc = m.vol[c];
         if (wantSignal) {
             f.signal[c] = (double)sig;
@@ -521,7 +522,7 @@ __global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gat
 template <typename T>
 __global__ void k_update(const DevMesh<T> m, Fields<T> f, const PhysD D, StageCoef sc) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n = m.n;
+    const int n = m.nU;
     if (c >= n) return;
     const double dt = *f.dt;
     const double vc = m.vol[c];
@@ -628,6 +629,26 @@ __global__ void k_copy(size_t cnt, const double *__restrict__ a, double *b) {
     for (; i < cnt; i += st) b[i] = a[i];
 }
 
+// ------------------------------------------------------------------ halo records (partitioned runs)
+// out[k * stride + v] = rec[cells[k] * stride + v]: the records of the cells another part needs
+template <typename T>
+__global__ void k_halo_pack(const T *__restrict__ rec, int stride, const int32_t *__restrict__ cells, int cnt,
+                            T *__restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)cnt * stride) return;
+    const size_t k = i / stride, v = i - k * stride;
+    out[i] = rec[(size_t)cells[k] * stride + v];
+}
+// rec[cells[k] * stride + v] = in[k * stride + v]: the ghosts' records received from their parts
+template <typename T>
+__global__ void k_halo_unpack(T *__restrict__ rec, int stride, const int32_t *__restrict__ cells, int cnt,
+                              const T *__restrict__ in) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)cnt * stride) return;
+    const size_t k = i / stride, v = i - k * stride;
+    rec[(size_t)cells[k] * stride + v] = in[i];
+}
+
 // ------------------------------------------------------------------ launchers
 constexpr int kGatherThreads = FG_GATHER_THREADS;
 int flux_blocks(int n) { return (n + kGatherThreads - 1) / kGatherThreads; }
@@ -657,7 +678,7 @@ int stage_kernels_setup(const DevMesh<T> &m) {
 }
 template <typename T>
 void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cudaStream_t s) {
-    const int nb = (m.n + m.blockCells - 1) / m.blockCells;
+    const int nb = (m.nU + m.blockCells - 1) / m.blockCells;
     if (P.limiter == 1)
         k_grad<T, 1><<<nb, m.blockCells, grad_smem(m), s>>>(m, f.Win, f.G, P);
     else
@@ -670,14 +691,28 @@ void launch_face(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, int
 template <typename T>
 void launch_gather(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, int mode, int wantSignal,
                    StageCoef sc, cudaStream_t s) {
-    k_gather<T><<<flux_blocks(m.n), kGatherThreads, 0, s>>>(m, f, D, mode, wantSignal, sc);
+    k_gather<T><<<flux_blocks(m.nU), kGatherThreads, 0, s>>>(m, f, D, mode, wantSignal, sc);
 }
 template int stage_kernels_setup<float>(const DevMesh<float> &);
 template int stage_kernels_setup<double>(const DevMesh<double> &);
 template <typename T>
 void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, StageCoef sc, cudaStream_t s) {
-    k_update<T><<<(m.n + 255) / 256, 256, 0, s>>>(m, f, D, sc);
+    k_update<T><<<(m.nU + 255) / 256, 256, 0, s>>>(m, f, D, sc);
 }
+template <typename T>
+void launch_halo_pack(const T *rec, int stride, const int32_t *cells, int cnt, T *out, cudaStream_t s) {
+    const size_t tot = (size_t)cnt * stride;
+    if (tot) k_halo_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, stride, cells, cnt, out);
+}
+template <typename T>
+void launch_halo_unpack(T *rec, int stride, const int32_t *cells, int cnt, const T *in, cudaStream_t s) {
+    const size_t tot = (size_t)cnt * stride;
+    if (tot) k_halo_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, stride, cells, cnt, in);
+}
+template void launch_halo_pack<float>(const float *, int, const int32_t *, int, float *, cudaStream_t);
+template void launch_halo_pack<double>(const double *, int, const int32_t *, int, double *, cudaStream_t);
+template void launch_halo_unpack<float>(float *, int, const int32_t *, int, const float *, cudaStream_t);
+template void launch_halo_unpack<double>(double *, int, const int32_t *, int, const double *, cudaStream_t);
 template <typename T>
 void launch_prim(int n, const double *U, T *W, const PhysD &D, cudaStream_t s) {
     k_prim<T><<<(n + 255) / 256, 256, 0, s>>>(n, U, W, D);

@@ -8,7 +8,8 @@ namespace fg {
 // the lanes that work on the faces of one cell read contiguous words.
 template <typename T>
 struct DevMesh {
-    int n;              // cells
+    int n;              // cells with records (W, G): own cells, then the ghosts of a partitioned mesh
+    int nU;             // own cells: the first nU cells carry a state (U, U0, RHS rows) and are updated
     int nSlots;         // max faces per cell
     const int32_t *nbr;   // neighbour cell, or -bc (1..5) on a boundary slot, or INT32_MIN unused
     const int32_t *flags; // bits 0-2: faces of the cell; bit 3+k: cell owns the face of slot k
@@ -124,6 +125,11 @@ template <typename T>
 void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, StageCoef sc, cudaStream_t s);
 template <typename T>
 void launch_prim(int n, const double *U, T *W, const PhysD &D, cudaStream_t s);
+// partitioned runs: records (stride values each) of cells[0..cnt) to / from a contiguous buffer
+template <typename T>
+void launch_halo_pack(const T *rec, int stride, const int32_t *cells, int cnt, T *out, cudaStream_t s);
+template <typename T>
+void launch_halo_unpack(T *rec, int stride, const int32_t *cells, int cnt, const T *in, cudaStream_t s);
 // dt = min(cfl * min_blocks, maxDt) from blockMin[nBlocks]
 void launch_dt_finalize(const double *blockMin, int nBlocks, double cfl, double maxDt, double *dt, cudaStream_t s);
 int flux_blocks(int n);   // blocks of the gather kernel (= entries of blockMin)

@@ -39,6 +39,16 @@ struct Mesh {
     int nTet = 0, nPyr = 0, nPrism = 0, nHex = 0;
     // ---- device ordering ----
     std::vector<int32_t> new2old, old2new;
+    // ---- part of a partitioned mesh (partition_mesh): cells [0, nOwned) are the part's own,
+    // cells [nOwned, nElem) its ghosts (face neighbours owned by other parts) ----
+    int nOwned = -1;                       // -1: not partitioned, every cell owned
+    int nParts = 1, part = 0;
+    std::vector<int32_t> cellGlobal;       // reference (.neu) index in the whole mesh of each cell
+    // cells whose records go to / come from each part q: sendCells[sendStart[q] .. sendStart[q+1])
+    // (own cells), recvCells[recvStart[q] .. recvStart[q+1]) (ghosts), both in the whole mesh's
+    // device order, so that the k-th record part p sends to q is q's k-th ghost from p
+    std::vector<int32_t> sendStart, sendCells, recvStart, recvCells;
+    int owned() const { return nOwned < 0 ? nElem : nOwned; }
 };
 
 // Parse a Gambit neutral file with the reference's grammar (DP/translator.cu:3-354).
@@ -51,6 +61,9 @@ int finish_mesh_gpu(Mesh &m, const fg_mesh_opts &o, std::string &err);
 // parts shared by both paths
 int match_periodic(Mesh &m, const fg_mesh_opts &o, std::vector<int64_t> &unmatched, std::string &err);
 int finish_order_geometry(Mesh &m, const fg_mesh_opts &o, std::string &err);
+// Part `part` of `nParts` of a finished mesh: the cells of a contiguous range of its device
+// (space-filling-curve) order, their ghosts, the faces touching them and the halo lists.
+int partition_mesh(const Mesh &g, int nParts, int part, Mesh &l, std::string &err);
 
 }  // namespace fg
 

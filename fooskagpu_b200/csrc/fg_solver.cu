@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -137,9 +138,37 @@ struct fg_solver {
     DevBuf logX, logY, logCnt;
     long long logCap = 0;
     int n = 0, nSlots = 0;
+    int nU = 0;               // own cells: the state rows (n - nU ghosts on a partitioned mesh)
+    bool parted = false;      // built from one part of a partitioned mesh
+    fg_halo_ops halo{};       // the partitioned run's transport (fg_solver_set_halo)
+    void *haloSend = nullptr, *haloRecv = nullptr;
     int iStep = 0;
     uint64_t bytes = 0;
     virtual int init(const fg::Mesh &m) = 0;
+    // gradient pass only; face fluxes + gather (+ RK unless mode is the residual) only
+    virtual int gradients(cudaStream_t s) = 0;
+    virtual int flux(int mode, int wantSignal, int irk, int writeU0, cudaStream_t s) = 0;
+    // partitioned runs: send the own halo cells' records of `field` and receive the ghosts'
+    virtual int halo_exchange(int field, cudaStream_t s) = 0;
+    virtual void halo_bytes(int64_t *send, int64_t *recv) const = 0;
+    // gradient pass with the record exchanges a partitioned run needs around it: the ghosts'
+    // primitive records before (they changed in the last update / relaxation), their gradient
+    // records after (the face fluxes read both sides')
+    int gradients_halo(cudaStream_t s) {
+        int rc;
+        if (parted && (rc = halo_exchange(FG_HALO_W, s))) return rc;
+        if ((rc = gradients(s))) return rc;
+        if (parted && (rc = halo_exchange(FG_HALO_G, s))) return rc;
+        return FG_OK;
+    }
+    // combine a per-part scalar over the parts (no-op on an unpartitioned mesh)
+    int reduce(int op, double *v) {
+        if (!parted) return FG_OK;
+        if (!halo.allreduce)
+            return set_err(FG_ERR_ARG, "partitioned mesh: set the transport with fg_solver_set_halo first");
+        if (halo.allreduce(halo.ctx, op, v) != 0) return set_err(FG_ERR_CUDA, "partitioned run: allreduce failed");
+        return FG_OK;
+    }
     virtual int set_state(const double *U, cudaStream_t s) = 0;
     virtual int get_state(double *U, cudaStream_t s) = 0;
     virtual int compute_rhs(int wantSignal, cudaStream_t s) = 0;
@@ -217,6 +246,8 @@ struct SolverT : public fg_solver {
     DevBuf dFIdx, dFGeo, dSlotFace, dClosure, dFB;
     DevBuf dOrdFlag, dOrdCnt, dOrdOff, dOrder, dOrdTotal;   // relaxation cell ordering
     DevBuf dPred, dHullOk, dTcErr;                          // surrogate predictions
+    DevBuf dSendCells, dRecvCells;                          // halo lists of a partitioned mesh
+    std::vector<int32_t> sendStart, recvStart;
     int cur = 0;
     DevMesh<T> dm{};
     PhysT<T> P{};
@@ -242,6 +273,8 @@ struct SolverT : public fg_solver {
 
     int init(const fg::Mesh &m) override {
         n = m.nElem;
+        nU = m.owned();
+        parted = m.nOwned >= 0;
         nSlots = m.maxFaces;
         cellCenter.assign(m.cellCenter.begin(), m.cellCenter.end());
         FG_CUDA_TRY(cudaSetDevice(device));
@@ -323,9 +356,10 @@ struct SolverT : public fg_solver {
         for (int i = 0; i < n; i++) {
             const int o = m.new2old[i];
             const fg::ElemType *et = fg::elem_type_for_nodes(m.elNN[o]);
-            int fl = et->nFaces;
             vol[i] = m.volume[o];
             volP[i] = pow(m.volume[o], 0.3333);
+            if (i >= nU) continue;   // a ghost: records only, no faces of its own
+            int fl = et->nFaces;
             for (int k = 0; k < et->nFaces; k++) {
                 const int f = elFc2fc[(size_t)o * 6 + k];
                 const int side = elFcSide[(size_t)o * 6 + k];
@@ -361,14 +395,17 @@ struct SolverT : public fg_solver {
             flags[i] = fl;
         }
         // faces in GPU order: by owner cell (renumbered), then owner slot, so the owners of
-        // consecutive faces are consecutive cells
+        // consecutive faces are consecutive cells (a ghost owns the faces it shares with own cells
+        // where the whole mesh makes it the owner)
         std::vector<int32_t> gFace(nF, -1), slotFace(S, -1), fIdx(2 * (size_t)nF);
         int nG = 0;
         for (int i = 0; i < n; i++) {
             const int o = m.new2old[i];
-            const int nfc = flags[i] & 7;
-            for (int k = 0; k < nfc; k++)
-                if ((flags[i] >> (3 + k)) & 1) gFace[elFc2fc[(size_t)o * 6 + k]] = nG++;
+            const int nfc = fg::elem_type_for_nodes(m.elNN[o])->nFaces;
+            for (int k = 0; k < nfc; k++) {
+                const int f = elFc2fc[(size_t)o * 6 + k];
+                if (f >= 0 && elFcSide[(size_t)o * 6 + k] == 0) gFace[f] = nG++;
+            }
         }
         if (nG != nF) return set_err(FG_ERR_MESH, "internal: face ownership does not cover every face");
         // face geometry: 11 components (n[3], A, x_f - x_owner [3], x_f - x_nb [3], mean volume)
@@ -479,7 +516,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(cudaMemcpy(dSlotFace.p, slotFace.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dClosure.p, closure.data(), 3 * (size_t)n * sizeof(T), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemset(dFB.p, 0, (size_t)nF * FREC * sizeof(T)));
-        const size_t u = (size_t)n * NV * sizeof(double);
+        const size_t u = (size_t)nU * NV * sizeof(double);
         FG_CUDA_TRY(dU.alloc(u));
         FG_CUDA_TRY(dU0.alloc(u));
         FG_CUDA_TRY(dRHS.alloc(u));
@@ -515,6 +552,7 @@ struct SolverT : public fg_solver {
                           &dPred, &dHullOk, &dTcErr})
             bytes += b->bytes;
         dm.n = n;
+        dm.nU = nU;
         dm.nSlots = nSlots;
         dm.nbr = dNbr.as<int32_t>();
         dm.flags = dFlags.as<int32_t>();
@@ -540,6 +578,19 @@ struct SolverT : public fg_solver {
         }
         dm.slotFace = dSlotFace.as<int32_t>();
         dm.closure = dClosure.as<T>();
+        if (parted) {
+            sendStart = m.sendStart;
+            recvStart = m.recvStart;
+            FG_CUDA_TRY(dSendCells.alloc(std::max<size_t>(m.sendCells.size(), 1) * sizeof(int32_t)));
+            FG_CUDA_TRY(dRecvCells.alloc(std::max<size_t>(m.recvCells.size(), 1) * sizeof(int32_t)));
+            if (!m.sendCells.empty())
+                FG_CUDA_TRY(cudaMemcpy(dSendCells.p, m.sendCells.data(), m.sendCells.size() * sizeof(int32_t),
+                                       cudaMemcpyHostToDevice));
+            if (!m.recvCells.empty())
+                FG_CUDA_TRY(cudaMemcpy(dRecvCells.p, m.recvCells.data(), m.recvCells.size() * sizeof(int32_t),
+                                       cudaMemcpyHostToDevice));
+            bytes += dSendCells.bytes + dRecvCells.bytes;
+        }
         if (stage_kernels_setup<T>(dm) != 0)
             return set_err(FG_ERR_CUDA, "stage kernels need more shared memory than the device allows (halo " +
                                             std::to_string(maxHalo) + " cells)");
@@ -547,7 +598,7 @@ struct SolverT : public fg_solver {
     }
 
     int set_state(const double *U, cudaStream_t s) override {
-        for (int i = 0; i < n; i++) {
+        for (int i = 0; i < nU; i++) {
             const double *u = U + (size_t)i * NV;
             if (!state_ok_host(u))
                 return set_err(FG_ERR_NAN, "fg_set_state: cell " + std::to_string(i) +
@@ -555,22 +606,22 @@ struct SolverT : public fg_solver {
         }
         FG_CUDA_TRY(cudaStreamSynchronize(s));
         *hBad = 0;
-        FG_CUDA_TRY(cudaMemcpyAsync(dStage.p, U, (size_t)n * NV * sizeof(double), cudaMemcpyHostToDevice, s));
+        FG_CUDA_TRY(cudaMemcpyAsync(dStage.p, U, (size_t)nU * NV * sizeof(double), cudaMemcpyHostToDevice, s));
         prof_begin(FG_K_OTHER, s);
-        launch_scatter_state(n, dStage.as<double>(), dNew2Old.as<int32_t>(), dU.as<double>(), s);
+        launch_scatter_state(nU, dStage.as<double>(), dNew2Old.as<int32_t>(), dU.as<double>(), s);
         prof_end(s);
         prof_begin(FG_K_OTHER, s);
-        launch_prim<T>(n, dU.as<double>(), dW[cur].as<T>(), D, s);
+        launch_prim<T>(nU, dU.as<double>(), dW[cur].as<T>(), D, s);
         prof_end(s);
         FG_LAUNCH_CHECK("set_state");
         return FG_OK;
     }
     int get_state(double *U, cudaStream_t s) override {
         prof_begin(FG_K_OTHER, s);
-        launch_gather_state(n, dU.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), s);
+        launch_gather_state(nU, dU.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("get_state");
-        FG_CUDA_TRY(cudaMemcpyAsync(U, dStage.p, (size_t)n * NV * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FG_CUDA_TRY(cudaMemcpyAsync(U, dStage.p, (size_t)nU * NV * sizeof(double), cudaMemcpyDeviceToHost, s));
         FG_CUDA_TRY(cudaStreamSynchronize(s));
         return FG_OK;
     }
@@ -582,25 +633,72 @@ struct SolverT : public fg_solver {
         sc.neglectZ = (cs.neglectZ == 1);
         return sc;
     }
-    int compute_rhs(int wantSignal, cudaStream_t s) override {
+    int gradients(cudaStream_t s) override {
         Fields<T> f = fields(cur);
         prof_begin(FG_K_GRAD, s);
         launch_grad<T>(dm, f, P, s);
         prof_end(s);
+        FG_LAUNCH_CHECK("gradients");
+        return FG_OK;
+    }
+    int flux(int mode, int wantSignal, int irk, int writeU0, cudaStream_t s) override {
+        Fields<T> f = fields(cur);
         prof_begin(FG_K_FLUX, s);
         launch_face<T>(dm, f, P, wantSignal, s);
         prof_end(s);
         prof_begin(FG_K_GATHER, s);
-        launch_gather<T>(dm, f, D, FLUX_RHS, wantSignal, coef(0, 0), s);
+        launch_gather<T>(dm, f, D, mode, wantSignal, mode == FLUX_RHS ? coef(0, 0) : coef(irk, writeU0), s);
         prof_end(s);
-        FG_LAUNCH_CHECK("compute_rhs");
+        FG_LAUNCH_CHECK("flux");
+        if (mode != FLUX_RHS) cur ^= 1;
         return FG_OK;
+    }
+    int halo_exchange(int field, cudaStream_t s) override {
+        if (!halo.exchange)
+            return set_err(FG_ERR_ARG, "partitioned mesh: set the transport with fg_solver_set_halo first");
+        T *rec = (field == FG_HALO_W) ? dW[cur].as<T>() : dG.as<T>();
+        const int stride = (field == FG_HALO_W) ? WREC : GREC;
+        const int nSend = sendStart.back(), nRecv = recvStart.back();
+        prof_begin(FG_K_OTHER, s);
+        launch_halo_pack<T>(rec, stride, dSendCells.as<int32_t>(), nSend, static_cast<T *>(haloSend), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("halo pack");
+        FG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (halo.exchange(halo.ctx, field, (int64_t)stride * (int64_t)sizeof(T), s) != 0)
+            return set_err(FG_ERR_CUDA, "partitioned run: halo exchange failed");
+        prof_begin(FG_K_OTHER, s);
+        launch_halo_unpack<T>(rec, stride, dRecvCells.as<int32_t>(), nRecv, static_cast<const T *>(haloRecv), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("halo unpack");
+        return FG_OK;
+    }
+    void halo_bytes(int64_t *send, int64_t *recv) const override {
+        const int64_t rb = (int64_t)GREC * (int64_t)sizeof(T);   // the larger of the two records
+        *send = parted ? rb * sendStart.back() : 0;
+        *recv = parted ? rb * recvStart.back() : 0;
+    }
+    int compute_rhs(int wantSignal, cudaStream_t s) override {
+        int rc;
+        if ((rc = gradients_halo(s))) return rc;
+        return flux(FLUX_RHS, wantSignal, 0, 0, s);
     }
     int time_step(double *dtOut, cudaStream_t s) override {
         prof_begin(FG_K_DT, s);
-        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(n), cs.cfl, cs.maxDt, dScal.as<double>(), s);
+        launch_dt_finalize(dBlockMin.as<double>(), flux_blocks(nU), cs.cfl, cs.maxDt, dScal.as<double>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("time_step");
+        if (parted) {
+            // the whole mesh's dt: the minimum over the parts
+            double dt = 0;
+            FG_CUDA_TRY(cudaMemcpyAsync(&dt, dScal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+            FG_CUDA_TRY(cudaStreamSynchronize(s));
+            int rc = reduce(FG_REDUCE_MIN, &dt);
+            if (rc) return rc;
+            FG_CUDA_TRY(cudaMemcpyAsync(dScal.p, &dt, sizeof(double), cudaMemcpyHostToDevice, s));
+            FG_CUDA_TRY(cudaStreamSynchronize(s));
+            if (dtOut) *dtOut = dt;
+            return FG_OK;
+        }
         if (dtOut) {
             FG_CUDA_TRY(cudaMemcpyAsync(dtOut, dScal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
             FG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -609,7 +707,7 @@ struct SolverT : public fg_solver {
     }
     int init_rk(cudaStream_t s) override {
         prof_begin(FG_K_OTHER, s);
-        launch_copy_u0(n, dU.as<double>(), dU0.as<double>(), s);
+        launch_copy_u0(nU, dU.as<double>(), dU0.as<double>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("init_rk");
         return FG_OK;
@@ -624,19 +722,9 @@ struct SolverT : public fg_solver {
         return FG_OK;
     }
     int stage(int irk, int writeU0, cudaStream_t s) override {
-        Fields<T> f = fields(cur);
-        prof_begin(FG_K_GRAD, s);
-        launch_grad<T>(dm, f, P, s);
-        prof_end(s);
-        prof_begin(FG_K_FLUX, s);
-        launch_face<T>(dm, f, P, 0, s);
-        prof_end(s);
-        prof_begin(FG_K_GATHER, s);
-        launch_gather<T>(dm, f, D, FLUX_FUSED, 0, coef(irk, writeU0), s);
-        prof_end(s);
-        FG_LAUNCH_CHECK("stage");
-        cur ^= 1;
-        return FG_OK;
+        int rc;
+        if ((rc = gradients_halo(s))) return rc;
+        return flux(FLUX_FUSED, 0, irk, writeU0, s);
     }
     int relax(fg_relax_stats *st, cudaStream_t s) override {
         FG_CUDA_TRY(cudaMemsetAsync(dCnt.p, 0, 8 * sizeof(int32_t), s));
@@ -651,7 +739,7 @@ struct SolverT : public fg_solver {
         const RelaxOrder O{dOrdFlag.as<uint8_t>(), dOrdCnt.as<int32_t>(), dOrdOff.as<int32_t>(), dOrder.as<int32_t>(),
                            dOrdTotal.as<int32_t>(), dPred.as<float4>(), dHullOk.as<int32_t>(), dTcErr.as<int32_t>()};
         prof_begin(FG_K_RELAX, s);
-        const int k = launch_relax<T>(n, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), S, L, O, s);
+        const int k = launch_relax<T>(nU, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), S, L, O, s);
         prof_end(s);
         launches += k - 1;
         FG_LAUNCH_CHECK("relaxation");
@@ -676,10 +764,22 @@ struct SolverT : public fg_solver {
     int cons(int ivar, double *out, cudaStream_t s) override {
         double *o = dScal.as<double>() + 2;
         prof_begin(FG_K_CONS, s);
-        launch_cons(n, ivar, dU.as<double>(), dVol.as<double>(), dBlockMin.as<double>(), o, s);
+        launch_cons(nU, ivar, dU.as<double>(), dVol.as<double>(), dBlockMin.as<double>(), o, s);
         prof_end(s);
         launches++;  // two kernels
         FG_LAUNCH_CHECK("cons_calc");
+        if (parted) {
+            // the whole mesh's integral: the sum over the parts
+            double v = 0;
+            FG_CUDA_TRY(cudaMemcpyAsync(&v, o, sizeof(double), cudaMemcpyDeviceToHost, s));
+            FG_CUDA_TRY(cudaStreamSynchronize(s));
+            int rc = reduce(FG_REDUCE_SUM, &v);
+            if (rc) return rc;
+            FG_CUDA_TRY(cudaMemcpyAsync(o, &v, sizeof(double), cudaMemcpyHostToDevice, s));
+            FG_CUDA_TRY(cudaStreamSynchronize(s));
+            if (out) *out = v;
+            return FG_OK;
+        }
         if (out) {
             FG_CUDA_TRY(cudaMemcpyAsync(out, o, sizeof(double), cudaMemcpyDeviceToHost, s));
             FG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -713,30 +813,30 @@ struct SolverT : public fg_solver {
     }
     int field_vars(double *out) override {
         DevBuf dOut, dCp;
-        FG_CUDA_TRY(dOut.alloc((size_t)n * 13 * sizeof(double)));
+        FG_CUDA_TRY(dOut.alloc((size_t)nU * 13 * sizeof(double)));
         FG_CUDA_TRY(dCp.alloc(2 * sizeof(double)));
         FG_CUDA_TRY(cudaMemcpy(dCp.p, cs.Cp, 2 * sizeof(double), cudaMemcpyHostToDevice));
-        k_field_vars<T><<<(n + 255) / 256, 256>>>(n, dU.as<double>(), dG.as<T>(), dNew2Old.as<int32_t>(), D,
+        k_field_vars<T><<<(nU + 255) / 256, 256>>>(nU, dU.as<double>(), dG.as<T>(), dNew2Old.as<int32_t>(), D,
                                                   dCp.as<double>(), dOut.as<double>());
         FG_LAUNCH_CHECK("field_vars");
         launches++;
         FG_CUDA_TRY(cudaDeviceSynchronize());
-        FG_CUDA_TRY(cudaMemcpy(out, dOut.p, (size_t)n * 13 * sizeof(double), cudaMemcpyDeviceToHost));
+        FG_CUDA_TRY(cudaMemcpy(out, dOut.p, (size_t)nU * 13 * sizeof(double), cudaMemcpyDeviceToHost));
         return FG_OK;
     }
     int get_rhs(double *rhs) override {
-        launch_gather_state(n, dRHS.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), 0);
+        launch_gather_state(nU, dRHS.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), 0);
         FG_LAUNCH_CHECK("get_rhs");
-        FG_CUDA_TRY(cudaMemcpy(rhs, dStage.p, (size_t)n * NV * sizeof(double), cudaMemcpyDeviceToHost));
+        FG_CUDA_TRY(cudaMemcpy(rhs, dStage.p, (size_t)nU * NV * sizeof(double), cudaMemcpyDeviceToHost));
         return FG_OK;
     }
     int get_limited(double *grad, double *theta) override {
         FG_CUDA_TRY(cudaDeviceSynchronize());
-        std::vector<T> g((size_t)n * GREC);
-        std::vector<int32_t> n2o(n);
+        std::vector<T> g((size_t)nU * GREC);
+        std::vector<int32_t> n2o(nU);
         FG_CUDA_TRY(cudaMemcpy(g.data(), dG.p, g.size() * sizeof(T), cudaMemcpyDeviceToHost));
-        FG_CUDA_TRY(cudaMemcpy(n2o.data(), dNew2Old.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < n; i++) {
+        FG_CUDA_TRY(cudaMemcpy(n2o.data(), dNew2Old.p, (size_t)nU * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < nU; i++) {
             const size_t o = (size_t)n2o[i];
             for (int v = 0; v < NV; v++) {
                 if (theta) theta[o * NV + v] = (v < NP) ? (double)g[(size_t)i * GREC + v] : 0.0;
@@ -748,11 +848,11 @@ struct SolverT : public fg_solver {
     }
     int get_signal(double *sig) override {
         FG_CUDA_TRY(cudaDeviceSynchronize());
-        std::vector<double> h(n);
-        std::vector<int32_t> n2o(n);
-        FG_CUDA_TRY(cudaMemcpy(h.data(), dSig.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
-        FG_CUDA_TRY(cudaMemcpy(n2o.data(), dNew2Old.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < n; i++) sig[n2o[i]] = h[i];
+        std::vector<double> h(nU);
+        std::vector<int32_t> n2o(nU);
+        FG_CUDA_TRY(cudaMemcpy(h.data(), dSig.p, (size_t)nU * sizeof(double), cudaMemcpyDeviceToHost));
+        FG_CUDA_TRY(cudaMemcpy(n2o.data(), dNew2Old.p, (size_t)nU * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < nU; i++) sig[n2o[i]] = h[i];
         return FG_OK;
     }
 };
@@ -882,6 +982,46 @@ int fg_mesh_permutation(const fg_mesh *mm, int32_t *new2old, int32_t n) {
 
 void fg_mesh_free(fg_mesh *m) { delete m; }
 
+int fg_mesh_partition(const fg_mesh *mm, int32_t nParts, int32_t part, fg_mesh **out) {
+    if (!mm || !out) return set_err(FG_ERR_ARG, "fg_mesh_partition: null argument");
+    *out = nullptr;
+    std::unique_ptr<fg_mesh> l(new fg_mesh());
+    std::string err;
+    const int rc = fg::partition_mesh(mm->m, nParts, part, l->m, err);
+    if (rc != FG_OK) return set_err(rc, err);
+    *out = l.release();
+    return FG_OK;
+}
+int fg_mesh_partition_info(const fg_mesh *mm, fg_partition_info *info) {
+    if (!mm || !info) return set_err(FG_ERR_ARG, "fg_mesh_partition_info: null argument");
+    const fg::Mesh &m = mm->m;
+    info->nParts = m.nParts;
+    info->part = m.part;
+    info->nOwned = m.owned();
+    info->nGhost = m.nElem - m.owned();
+    info->nSend = m.sendStart.empty() ? 0 : m.sendStart.back();
+    info->nRecv = m.recvStart.empty() ? 0 : m.recvStart.back();
+    return FG_OK;
+}
+int fg_mesh_partition_maps(const fg_mesh *mm, int32_t *cellGlobal, int32_t *sendStart, int32_t *sendCells,
+                           int32_t *recvStart, int32_t *recvCells) {
+    if (!mm) return set_err(FG_ERR_ARG, "fg_mesh_partition_maps: null mesh");
+    const fg::Mesh &m = mm->m;
+    if (m.nOwned < 0) {
+        // a whole mesh: one part owning every cell, no halo
+        if (cellGlobal) std::iota(cellGlobal, cellGlobal + m.nElem, 0);
+        if (sendStart) sendStart[0] = sendStart[1] = 0;
+        if (recvStart) recvStart[0] = recvStart[1] = 0;
+        return FG_OK;
+    }
+    if (cellGlobal) std::copy(m.cellGlobal.begin(), m.cellGlobal.end(), cellGlobal);
+    if (sendStart) std::copy(m.sendStart.begin(), m.sendStart.end(), sendStart);
+    if (sendCells) std::copy(m.sendCells.begin(), m.sendCells.end(), sendCells);
+    if (recvStart) std::copy(m.recvStart.begin(), m.recvStart.end(), recvStart);
+    if (recvCells) std::copy(m.recvCells.begin(), m.recvCells.end(), recvCells);
+    return FG_OK;
+}
+
 int fg_solver_create(const fg_mesh *m, const fg_case *c, int32_t precision, int32_t device, fg_solver **out) {
     if (!m || !c || !out) return set_err(FG_ERR_ARG, "fg_solver_create: null argument");
     *out = nullptr;
@@ -918,6 +1058,22 @@ int fg_solver_destroy(fg_solver *s) {
 int fg_solver_memory(const fg_solver *s, uint64_t *bytes) {
     if (!s || !bytes) return set_err(FG_ERR_ARG, "fg_solver_memory: null argument");
     *bytes = s->bytes;
+    return FG_OK;
+}
+int fg_halo_buffer_bytes(const fg_solver *s, int64_t *sendBytes, int64_t *recvBytes) {
+    if (!s || !sendBytes || !recvBytes) return set_err(FG_ERR_ARG, "fg_halo_buffer_bytes: null argument");
+    s->halo_bytes(sendBytes, recvBytes);
+    return FG_OK;
+}
+int fg_solver_set_halo(fg_solver *s, const fg_halo_ops *ops, void *sendBuf, void *recvBuf) {
+    if (!s || !ops || !ops->exchange || !ops->allreduce) return set_err(FG_ERR_ARG, "fg_solver_set_halo: null argument");
+    if (!s->parted) return set_err(FG_ERR_ARG, "fg_solver_set_halo: the solver's mesh is not a part (fg_mesh_partition)");
+    int64_t sb = 0, rb = 0;
+    s->halo_bytes(&sb, &rb);
+    if ((sb > 0 && !sendBuf) || (rb > 0 && !recvBuf)) return set_err(FG_ERR_ARG, "fg_solver_set_halo: null buffer");
+    s->halo = *ops;
+    s->haloSend = sendBuf;
+    s->haloRecv = recvBuf;
     return FG_OK;
 }
 
@@ -1047,12 +1203,12 @@ struct CkHeader {
 int fg_checkpoint_write(fg_solver *s, const char *path) {
     FG_ENTER(s);
     if (!path) return set_err(FG_ERR_ARG, "fg_checkpoint_write: null path");
-    std::vector<double> U((size_t)s->n * fg::NV);
+    std::vector<double> U((size_t)s->nU * fg::NV);
     int rc = s->get_state(U.data(), 0);
     if (rc != FG_OK) return rc;
     CkHeader h{};
     std::memcpy(h.magic, kCkMagic, 8);
-    h.nElem = s->n;
+    h.nElem = s->nU;
     h.neq = fg::NV;
     h.iStep = s->iStep;
     h.precision = s->precision;
@@ -1071,12 +1227,12 @@ int fg_checkpoint_read(fg_solver *s, const char *path) {
     FILE *fp = fopen(path, "rb");
     if (!fp) return set_err(FG_ERR_IO, std::string("fg_checkpoint_read: cannot open ") + path);
     CkHeader h{};
-    std::vector<double> U((size_t)s->n * fg::NV);
+    std::vector<double> U((size_t)s->nU * fg::NV);
     bool ok = fread(&h, sizeof(h), 1, fp) == 1 && std::memcmp(h.magic, kCkMagic, 8) == 0;
-    if (ok && (h.nElem != s->n || h.neq != fg::NV)) {
+    if (ok && (h.nElem != s->nU || h.neq != fg::NV)) {
         fclose(fp);
         return set_err(FG_ERR_ARG, "fg_checkpoint_read: checkpoint is for " + std::to_string(h.nElem) +
-                                       " cells, the solver has " + std::to_string(s->n));
+                                       " cells, the solver has " + std::to_string(s->nU));
     }
     ok = ok && fread(U.data(), sizeof(double), U.size(), fp) == U.size();
     fclose(fp);
@@ -1093,17 +1249,17 @@ int fg_field_dump(fg_solver *s, const char *path) {
     FG_ENTER(s);
     if (!path) return set_err(FG_ERR_ARG, "fg_field_dump: null path");
     const double *cellCenter = s->cellCenter.data();
-    std::vector<double> v((size_t)s->n * 13);
+    std::vector<double> v((size_t)s->nU * 13);
     int rc = s->field_vars(v.data());
     if (rc != FG_OK) return rc;
-    for (int i = 0; i < s->n; i++)
+    for (int i = 0; i < s->nU; i++)
         for (int d = 0; d < 3; d++) v[(size_t)i * 13 + d] = cellCenter[(size_t)i * 3 + d];
     double t = 0, dt = 0;
     rc = s->get_time(&dt, &t);
     if (rc != FG_OK) return rc;
     FILE *fp = fopen(path, "wb");
     if (!fp) return set_err(FG_ERR_IO, std::string("fg_field_dump: cannot open ") + path);
-    const int32_t hdr[4] = {s->n, 13, s->iStep, 0};
+    const int32_t hdr[4] = {s->nU, 13, s->iStep, 0};
     const bool ok = fwrite(kFdMagic, 1, 8, fp) == 8 && fwrite(hdr, sizeof(hdr), 1, fp) == 1 &&
                     fwrite(&t, sizeof(double), 1, fp) == 1 && fwrite(v.data(), sizeof(double), v.size(), fp) == v.size();
     if (fclose(fp) != 0 || !ok) return set_err(FG_ERR_IO, std::string("fg_field_dump: write failed: ") + path);

@@ -178,6 +178,54 @@ int  fg_mesh_view_get(const fg_mesh *m, fg_mesh_view *view);
 int  fg_mesh_permutation(const fg_mesh *m, int32_t *new2old, int32_t n);
 void fg_mesh_free(fg_mesh *m);
 
+/* ---------------------------------------------------------------- partitioned runs
+ * Replace the reference's METIS decomposition, local-mesh build and per-stage halo
+ * communication (DP/decompose.cu:52, DP/buildLocalMesh.cu, DP/communicate.cu) for runs with one
+ * GPU per part.  Part p of P owns the cells of the contiguous range [n p / P, n (p+1) / P) of the
+ * mesh's device order (the Morton order of the cell centres: a compact region) and holds one
+ * layer of ghost cells, its face neighbours in other parts.  The part mesh keeps every face that
+ * touches an own cell with the whole mesh's orientation, geometry and boundary code.
+ *
+ * fg_mesh_partition: part `part` of `nParts` of a loaded mesh, as a new mesh handle whose cells
+ * are the own cells (device order) followed by the ghosts.  A solver created on it takes and
+ * returns the state of the own cells only (fg_set_state / fg_get_state: nOwned rows, in that
+ * order), and needs a transport (fg_solver_set_halo) before its first stage. */
+int fg_mesh_partition(const fg_mesh *m, int32_t nParts, int32_t part, fg_mesh **out);
+typedef struct fg_partition_info {
+    int32_t nParts, part;   /* 1, 0 for a mesh that is not a part                     */
+    int32_t nOwned;         /* own cells: the first nOwned cells of the part mesh      */
+    int32_t nGhost;         /* ghost cells, after the own ones                         */
+    int32_t nSend, nRecv;   /* entries of the send / receive lists over all parts      */
+} fg_partition_info;
+int fg_mesh_partition_info(const fg_mesh *m, fg_partition_info *info);
+/* cellGlobal[nOwned + nGhost]: .neu index in the whole mesh of each cell of the part;
+ * sendStart[nParts + 1], sendCells[nSend]: the own cells whose records go to part q are
+ * sendCells[sendStart[q] .. sendStart[q+1]); recvStart / recvCells the same for the ghosts whose
+ * records come from part q.  Both lists follow the whole mesh's device order, so the k-th record
+ * part p sends to q is q's k-th ghost from p.  Any pointer may be NULL. */
+int fg_mesh_partition_maps(const fg_mesh *m, int32_t *cellGlobal, int32_t *sendStart, int32_t *sendCells,
+                           int32_t *recvStart, int32_t *recvCells);
+
+/* Transport of a partitioned run (the caller's NCCL / MPI / shared memory).  Per RK stage the
+ * solver exchanges the primitive records (FG_HALO_W) of the halo cells before the gradient pass
+ * and their gradient records (FG_HALO_G) after it; the dt (every adaptDtItr steps) and the
+ * conservation integral are combined with allreduce.
+ *   exchange(ctx, field, recordBytes, stream): when called, sendBuf holds the nSend records of
+ *     `field` (recordBytes each, in send-list order) and every earlier kernel on `stream` has
+ *     finished.  The callee sends records [sendStart[q], sendStart[q+1]) to part q, receives part
+ *     q's into records [recvStart[q], recvStart[q+1]) of recvBuf for every q, and returns 0 once
+ *     recvBuf is complete (readable by work enqueued on `stream` afterwards).
+ *   allreduce(ctx, op, value): combine *value over the parts (op FG_REDUCE_MIN / FG_REDUCE_SUM) in
+ *     place; 0 on success.
+ * sendBuf / recvBuf: device buffers of at least the sizes fg_halo_buffer_bytes gives. */
+enum fg_halo_field { FG_HALO_W = 0, FG_HALO_G = 1 };
+enum fg_reduce_op { FG_REDUCE_MIN = 0, FG_REDUCE_SUM = 1 };
+typedef struct fg_halo_ops {
+    void *ctx;
+    int (*exchange)(void *ctx, int32_t field, int64_t recordBytes, void *stream);
+    int (*allreduce)(void *ctx, int32_t op, double *value);
+} fg_halo_ops;
+
 /* ---------------------------------------------------------------- solver context
  * Replaces startDevice (DP/startDevice.cu:14): allocates every device array once. */
 typedef struct fg_solver fg_solver;
@@ -192,6 +240,10 @@ int fg_solver_create(const fg_mesh *m, const fg_case *c, int32_t precision, int3
 int fg_solver_destroy(fg_solver *s);
 /* Device bytes held by the solver (mesh + field arrays). */
 int fg_solver_memory(const fg_solver *s, uint64_t *bytes);
+/* Partitioned runs: device bytes the send / receive buffers of fg_solver_set_halo need (0 on a
+ * solver of a whole mesh), and the transport with those buffers. */
+int fg_halo_buffer_bytes(const fg_solver *s, int64_t *sendBytes, int64_t *recvBytes);
+int fg_solver_set_halo(fg_solver *s, const fg_halo_ops *ops, void *sendBuf, void *recvBuf);
 
 /* Replaces initialize / readField (DP/initialize.cu:61, DP/restart.cu:424): upload U
  * (nElem*10 doubles, reference order) from host memory.  stream may be NULL. */

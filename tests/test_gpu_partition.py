@@ -1,0 +1,66 @@
+"""Partitioned runs (one part per GPU in production) against the whole-mesh run, with the parts
+as threads on one GPU exchanging their halo records through device copies (tests/halo_threads.py).
+Each part computes its own cells' gradients, the fluxes of every face of its own cells (a face
+on a part border is computed by both parts from the same records) and the updates, so the state
+after full explicitLoop steps (adaptive dt combined over the parts, relaxation) must equal the
+whole-mesh run's bit for bit, in both precisions, for 2 and 3 parts."""
+import numpy as np
+import pytest
+
+from gpu_cases import make
+from halo_threads import ThreadGroup, ThreadHalo, run_parts
+from fooskagpu_b200.api import Solver
+
+pytestmark = pytest.mark.gpu
+STEPS = 5
+
+
+def _whole(m, c, U, prec):
+    s = Solver(m, c, precision=prec)
+    s.set_state(U)
+    for _ in range(STEPS):
+        s.step()
+    out = s.get_state(), s.time(), s.cons_calc(1)
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("name,P", [("tet_ref", 2), ("tet_ref", 3), ("hex_periodic_tgv", 2),
+                                    ("mixed_ref_rk3", 3), ("tet_ext", 2)])
+def test_partitioned_matches_whole_mesh(name, P, prec, meshdir):
+    m, c, U = make(name, meshdir, prec)
+    Uw, tw, cw = _whole(m, c, U, prec)
+    parts = [m.partition(P, p) for p in range(P)]
+    group = ThreadGroup(P)
+    solvers = [Solver(pm, c, precision=prec) for pm in parts]
+    halos = [ThreadHalo(group, s, pm) for s, pm in zip(solvers, parts)]
+    own = [pm.partition_maps()["cell_global"][:pm.n_owned] for pm in parts]
+    for s, cg in zip(solvers, own):
+        s.set_state(U[cg])
+
+    def run(p):
+        for _ in range(STEPS):
+            solvers[p].step()
+        return solvers[p].get_state(), solvers[p].time(), solvers[p].cons_calc(1)
+
+    res = run_parts(run, group)
+    for p in range(P):
+        Up, tp, cp = res[p]
+        assert np.array_equal(Up, Uw[own[p]]), (p, np.abs(Up - Uw[own[p]]).max())
+        assert tp == tw
+        assert abs(cp - cw) <= 1e-13 * abs(cw)
+        assert halos[p].exchanges == 2 * c.rkSteps * STEPS
+    for s in solvers:
+        s.close()
+
+
+def test_part_solver_needs_a_transport(meshdir):
+    from fooskagpu_b200._lib import FgError
+    m, c, U = make("tet_ref", meshdir, "fp64")
+    pm = m.partition(2, 0)
+    s = Solver(pm, c, precision="fp64")
+    s.set_state(U[pm.partition_maps()["cell_global"][:pm.n_owned]])
+    with pytest.raises(FgError, match="fg_solver_set_halo"):
+        s.step()
+    s.close()
