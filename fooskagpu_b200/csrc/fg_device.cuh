@@ -200,9 +200,10 @@ __device__ __forceinline__ void hllc_flux(const PhysT<T> &P, const T *L, const T
     pF = pm;
 }
 
-// WALE eddy viscosity (DP/computeViscousStresses.cu:3-60) for g = grad u (row i = component).
+// WALE eddy viscosity (DP/computeViscousStresses.cu:3-60) for g = grad u (row i = component);
+// lsSq = Ls^2 = (0.325 Vavg^0.3333333333333)^2, precomputed per face on the host in FP64.
 template <typename T>
-__device__ __forceinline__ T wale_nu(const T *g, T volAvg) {
+__device__ __forceinline__ T wale_nu(const T *g, T lsSq) {
     T sq[9];
 #pragma unroll
     for (int i = 0; i < 3; i++)
@@ -223,8 +224,7 @@ __device__ __forceinline__ T wale_nu(const T *g, T volAvg) {
     T num = s1 * r1;                       // s1^1.5
     const T den = s1 * sqrt(r1) + s2 * s2 * r2 + (T)1e-12;  // s1^1.25 + s2^2.5 + 1e-12
     if (den < (T)1e-10) num = 0;
-    const T Ls = (T)0.325 * cbrt(volAvg);
-    return Ls * Ls * num / den;
+    return lsSq * num / den;
 }
 
 }  // namespace fg

@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(co
         T gv[9];
 #pragma unroll
         for (int q = 0; q < 9; q++) gv[q] = (gO[q] + gN[q]) * (T)0.5;
-        const T nut = P.turb ? wale_nu(gv, m.fVavg[fi]) : (T)0;
+        const T nut = P.turb ? wale_nu(gv, m.fLsSq[fi]) : (T)0;
         const T dv = (gv[0] + gv[4] + gv[8]) * ((T)2 / 3);
         const T t00 = 2 * gv[0] - dv, t11 = 2 * gv[4] - dv, t22 = 2 * gv[8] - dv;
         const T t01 = gv[1] + gv[3], t02 = gv[2] + gv[6], t12 = gv[5] + gv[7];

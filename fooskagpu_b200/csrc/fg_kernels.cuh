@@ -39,7 +39,8 @@ struct DevMesh {
     const T *fnx, *fny, *fnz, *fA;   // canonical unit normal (owner -> neighbour) and area
     const T *fdo[3];                 // face centre - owner centre
     const T *fdn[3];                 // face centre - neighbour centre (periodic image)
-    const T *fVavg;                  // (V_owner + V_neighbour) / 2, V_owner on a boundary face
+    const T *fLsSq;                  // WALE Ls^2 = (0.325 Vavg^0.3333333333333)^2, Vavg = (V_owner +
+                                     // V_neighbour) / 2, V_owner on a boundary face
     const int32_t *slotFace;         // [c * nSlots + k] face of a cell slot
     const T *closure;                // [3][n] sum over the cell's faces of outward n * A
 };

@@ -408,7 +408,7 @@ struct SolverT : public fg_solver {
             }
         }
         if (nG != nF) return set_err(FG_ERR_MESH, "internal: face ownership does not cover every face");
-        // face geometry: 11 components (n[3], A, x_f - x_owner [3], x_f - x_nb [3], mean volume)
+        // face geometry: 11 components (n[3], A, x_f - x_owner [3], x_f - x_nb [3], WALE Ls^2)
         const size_t FS = ((size_t)nF * sizeof(T) + 15) / 16 * 16 / sizeof(T);
         std::vector<T> fgeo(11 * FS, (T)0);
         for (int f = 0; f < nF; f++) {
@@ -426,7 +426,10 @@ struct SolverT : public fg_solver {
                     fgeo[(size_t)(7 + d) * FS + g] =
                         (T)((xf + m.nbShift[(size_t)f * 3 + d]) - m.cellCenter[(size_t)nbo * 3 + d]);
             }
-            fgeo[10 * FS + g] = (T)((bc == 0) ? (m.volume[own] + m.volume[nbo]) * 0.5 : m.volume[own]);
+            // WALE length scale squared of the face (DP/computeViscousStresses.cu:54-56)
+            const double vAvg = (bc == 0) ? (m.volume[own] + m.volume[nbo]) * 0.5 : m.volume[own];
+            const double ls = 0.325 * pow(vAvg, 0.3333333333333);
+            fgeo[10 * FS + g] = (T)(ls * ls);
         }
         // slot -> face, and each cell's sum of outward n A (closes to rounding on a closed cell)
         std::vector<double> clo(3 * (size_t)n, 0.0);
@@ -574,7 +577,7 @@ struct SolverT : public fg_solver {
                 dm.fdo[d] = fg + (4 + d) * FS;
                 dm.fdn[d] = fg + (7 + d) * FS;
             }
-            dm.fVavg = fg + 10 * FS;
+            dm.fLsSq = fg + 10 * FS;
         }
         dm.slotFace = dSlotFace.as<int32_t>();
         dm.closure = dClosure.as<T>();
