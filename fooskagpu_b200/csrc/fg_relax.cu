@@ -458,8 +458,20 @@ struct InRelax {
     }
 };
 
+// resident blocks asked of the compiler for the thermal-only instantiation (kOrd false): its
+// FP64 Newton is latency-bound; 6 blocks of 128 threads (80 registers, a few spilled) measured
+// 0.180 -> 0.150 ms early and 0.461 -> 0.400 ms later in the 128^3 TGV against 4 blocks
+#ifndef FG_THERM_MINBLOCKS
+#define FG_THERM_MINBLOCKS 6
+#endif
+// the same for the chemical-first instantiations (kOrd true: Gibbs and thermal Newton): 4 blocks
+// (128 registers, a few spilled, against 156-196 uncapped) measured 2.81 -> 1.99 ms (FP64 Newton)
+// and 0.81 -> 0.66 ms (surrogate + polish) per relaxation on the 96^3 two-phase workload
+#ifndef FG_CHEM_MINBLOCKS
+#define FG_CHEM_MINBLOCKS 4
+#endif
 template <typename T, bool kSG, bool kLog, bool kOrd>
-__global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R,
+__global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBLOCKS) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R,
                                                int32_t *counters, const SurrogateDev S, const RelaxLog Lg,
                                                const int32_t *order, const int32_t *nChem, const float4 *pred,
                                                const int32_t *hullOk) {
@@ -474,7 +486,9 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
     if (act) {
 #pragma unroll
         for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
-        if (R.chemFlag == 1) chem = kOrd ? (i < *nChem) : needs_chem(R, h, u);
+        // kOrd: cells ordered chemical-first (chemFlag == 1); otherwise every cell is thermal
+        // (chemFlag != 1), and the chemical solver is compiled out of this instantiation
+        if (kOrd) chem = i < *nChem;
         if (chem && (kSG || kLog)) {
             chem_mixture(R, u, &rm, &re, &ag);
             // the network's prediction for this cell (k_sg_tc over the chemical cells) if its
@@ -490,7 +504,7 @@ __global__ void __launch_bounds__(128) k_relax(int n, double *U, T *W, const Phy
             used = chem_polish(R, h, u, pr, rm, re, S.relTol, S.polishIters, &pits);
         }
         if (!used) {
-            ab = chem ? chem_cell(R, h, u, &its) : therm_cell(R, h, u, &its);
+            ab = (kOrd && chem) ? chem_cell(R, h, u, &its) : therm_cell(R, h, u, &its);
             if (kLog && chem && !ab) {
                 // training sample: (rho, e, Y) before the solve -> (p, T, alpha, Y_eq) after it
                 const unsigned long long k = atomicAdd(Lg.count, 1ULL);
