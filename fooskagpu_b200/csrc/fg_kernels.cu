@@ -608,6 +608,22 @@ __global__ void k_cons_final(const double *blockSum, int nb, double *out) {
     if (threadIdx.x == 0) *out = sh[0];
 }
 
+// ------------------------------------------------------------------ uploaded state check
+// firstBad = min over cells c of an AoS state Ua[c * 10 + v] that is not usable: a non-finite
+// sum, alpha outside [0, 1] (beyond 1e-9) or a negative partial density (the order-independent
+// minimum reports the first such cell in the caller's order)
+__global__ void k_check_state(int n, const double *__restrict__ Ua, int32_t *firstBad) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double *u = Ua + (size_t)c * NV;
+    double sum = 0;
+#pragma unroll
+    for (int v = 0; v < NV; v++) sum += u[v];
+    const bool ok = isfinite(sum) && u[0] >= -1e-9 && u[0] <= 1.0 + 1e-9 && u[1] >= 0.0 && u[2] >= 0.0 &&
+                    u[1] + u[2] > 0.0;
+    if (!ok) atomicMin(firstBad, c);
+}
+
 // ------------------------------------------------------------------ state layout conversion
 __global__ void k_scatter_state(int n, const double *__restrict__ Ua, const int32_t *__restrict__ new2old, double *U) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -724,6 +740,11 @@ void launch_cons(int n, int ivar, const double *U, const double *vol, double *bl
     const int nb = cons_blocks(n);
     k_cons_blocks<<<nb, kConsThreads, 0, s>>>(n, ivar, U, vol, blockSum);
     k_cons_final<<<1, 1024, 0, s>>>(blockSum, nb, out);
+}
+void launch_check_state(int n, const double *Ua, int32_t *firstBad, cudaStream_t s) {
+    static const int32_t none = INT_MAX;
+    cudaMemcpyAsync(firstBad, &none, sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    if (n > 0) k_check_state<<<(n + 255) / 256, 256, 0, s>>>(n, Ua, firstBad);
 }
 void launch_scatter_state(int n, const double *Ua, const int32_t *new2old, double *U, cudaStream_t s) {
     k_scatter_state<<<(n + 255) / 256, 256, 0, s>>>(n, Ua, new2old, U);

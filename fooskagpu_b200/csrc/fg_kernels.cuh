@@ -170,6 +170,8 @@ int launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, i
 void launch_cons(int n, int ivar, const double *U, const double *vol, double *blockSum, double *out, cudaStream_t s);
 int cons_blocks(int n);
 
+// first cell of an uploaded AoS state (n x 10) that is not usable, INT_MAX if none
+void launch_check_state(int n, const double *Uaos, int32_t *firstBad, cudaStream_t s);
 // reference-order AoS <-> renumbered SoA
 void launch_scatter_state(int n, const double *Uaos, const int32_t *new2old, double *U, cudaStream_t s);
 void launch_gather_state(int n, const double *U, const int32_t *new2old, double *Uaos, cudaStream_t s);

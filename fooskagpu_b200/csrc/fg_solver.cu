@@ -192,14 +192,6 @@ struct fg_solver {
 
 namespace fg {
 
-// an uploaded state: finite, alpha in [0, 1] (within 1e-9), partial densities not negative
-inline bool state_ok_host(const double *u) {
-    double sum = 0;
-    for (int v = 0; v < NV; v++) sum += u[v];
-    return std::isfinite(sum) && u[0] >= -1e-9 && u[0] <= 1.0 + 1e-9 && u[1] >= 0.0 && u[2] >= 0.0 &&
-           u[1] + u[2] > 0.0;
-}
-
 __global__ void k_advance_time(const double *dt, double *t) { *t += *dt; }
 
 // export variables of DP/export_plt.cu:42-80 per cell (not averaged to the nodes): x y z avfL avfG
@@ -247,6 +239,7 @@ struct SolverT : public fg_solver {
     DevBuf dOrdFlag, dOrdCnt, dOrdOff, dOrder, dOrdTotal;   // relaxation cell ordering
     DevBuf dPred, dHullOk, dTcErr;                          // surrogate predictions
     DevBuf dSendCells, dRecvCells;                          // halo lists of a partitioned mesh
+    DevBuf dChk;                                            // set_state: first unusable cell
     std::vector<int32_t> sendStart, recvStart;
     int cur = 0;
     DevMesh<T> dm{};
@@ -531,6 +524,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n), cons_blocks(n)) * sizeof(double)));
         FG_CUDA_TRY(dScal.alloc(4 * sizeof(double)));   // dt, time, cons
         FG_CUDA_TRY(dCnt.alloc(8 * sizeof(int32_t)));
+        FG_CUDA_TRY(dChk.alloc(sizeof(int32_t)));
         FG_CUDA_TRY(dOrdFlag.alloc((size_t)n));
         FG_CUDA_TRY(dOrdCnt.alloc((size_t)relax_order_blocks(n) * sizeof(int32_t)));
         FG_CUDA_TRY(dOrdOff.alloc((size_t)relax_order_blocks(n) * sizeof(int32_t)));
@@ -601,15 +595,20 @@ struct SolverT : public fg_solver {
     }
 
     int set_state(const double *U, cudaStream_t s) override {
-        for (int i = 0; i < nU; i++) {
-            const double *u = U + (size_t)i * NV;
-            if (!state_ok_host(u))
-                return set_err(FG_ERR_NAN, "fg_set_state: cell " + std::to_string(i) +
-                                               " is not finite or has alpha outside [0, 1] or a negative partial density");
-        }
         FG_CUDA_TRY(cudaStreamSynchronize(s));
-        *hBad = 0;
         FG_CUDA_TRY(cudaMemcpyAsync(dStage.p, U, (size_t)nU * NV * sizeof(double), cudaMemcpyHostToDevice, s));
+        // checked on the device before it replaces the state (only the staging buffer so far)
+        prof_begin(FG_K_OTHER, s);
+        launch_check_state(nU, dStage.as<double>(), dChk.as<int32_t>(), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("set_state check");
+        int32_t bad = 0;
+        FG_CUDA_TRY(cudaMemcpyAsync(&bad, dChk.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        FG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (bad != INT_MAX)
+            return set_err(FG_ERR_NAN, "fg_set_state: cell " + std::to_string(bad) +
+                                           " is not finite or has alpha outside [0, 1] or a negative partial density");
+        *hBad = 0;
         prof_begin(FG_K_OTHER, s);
         launch_scatter_state(nU, dStage.as<double>(), dNew2Old.as<int32_t>(), dU.as<double>(), s);
         prof_end(s);

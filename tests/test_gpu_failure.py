@@ -27,6 +27,14 @@ def test_set_state_rejects_bad_states(meshdir):
         assert e.value.code == FG_ERR_NAN
     s.set_state(U)
     assert s.check_state() == -1
+    # the first unusable cell in the caller's order is named, and a rejected upload leaves the
+    # state as it was
+    V = U.copy()
+    V[9, 1] = -2.0
+    V[4, 5] = np.inf
+    with pytest.raises(FgError, match="cell 4 "):
+        s.set_state(V)
+    assert np.array_equal(s.get_state(), U)
     s.close()
 
 
