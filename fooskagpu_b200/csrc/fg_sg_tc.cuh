@@ -23,7 +23,8 @@ constexpr int TC_W3 = TC_W2 + 64 * 64 * 2;     // W3: N 64 x K 64               
 constexpr int TC_W4 = TC_W3 + 64 * 64 * 2;     // W4: N 16 x K 64 (4 used)           2 KB
 constexpr int TC_WBYTES = TC_W4 + 16 * 64 * 2; // packed weights (bytes)
 constexpr int TC_A = TC_WBYTES;                // activations: 128 x K 64            16 KB
-constexpr int TC_BAR = TC_A + TC_M * 64 * 2;   // mbarrier (8 B) + TMEM address (4 B)
+constexpr int TC_BIAS = TC_A + TC_M * 64 * 2;  // hidden-layer biases, FP32 3 x 64    768 B
+constexpr int TC_BAR = TC_BIAS + 3 * 64 * 4;   // mbarrier (8 B) + TMEM address (4 B)
 constexpr int TC_SMEM = TC_BAR + 16;
 constexpr uint32_t TC_TMEM_COLS = 64;
 
@@ -92,8 +93,13 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-__device__ __forceinline__ void tc_store_bf16(unsigned char *smA, int row, int k, float x) {
-    *reinterpret_cast<__nv_bfloat16 *>(smA + tc_smem_off(row, k, TC_M)) = __float2bfloat16_rn(x);
+// row `row`, columns k0 .. k0 + 7 (k0 a multiple of 8) of the A operand: 8 consecutive BF16 of
+// one core-matrix row, one 16-byte store
+__device__ __forceinline__ void tc_store8_bf16(unsigned char *smA, int row, int k0, const float *x) {
+    __nv_bfloat162 p[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) p[q] = __floats2bfloat162_rn(x[2 * q], x[2 * q + 1]);   // x[2q] in the low half
+    *reinterpret_cast<uint4 *>(smA + tc_smem_off(row, k0, TC_M)) = *reinterpret_cast<const uint4 *>(p);
 }
 
 // One layer on the tensor cores: D[128 x n] = A[128 x 16 kSlabs] * W^T, into TMEM; returns false
@@ -134,6 +140,12 @@ __global__ void __launch_bounds__(128) k_sg_tc(const SurrogateDev S, const unsig
     const int t = threadIdx.x;
     for (int q = t; q < TC_WBYTES / 16; q += blockDim.x)
         reinterpret_cast<uint4 *>(sm)[q] = reinterpret_cast<const uint4 *>(wpack)[q];
+    {
+        // the three hidden layers' biases, read by every thread of a tile (broadcast)
+        float *b = reinterpret_cast<float *>(sm + TC_BIAS);
+        for (int q = t; q < 3 * 64; q += blockDim.x)
+            b[q] = __ldg(S.params + (q < 64 ? SG_OFF_B1 + q : (q < 128 ? SG_OFF_B2 + q - 64 : SG_OFF_B3 + q - 128)));
+    }
     const uint32_t bar = tc_smem_addr(sm + TC_BAR);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + TC_BAR + 8);
     if (t == 0) {
@@ -166,20 +178,30 @@ __global__ void __launch_bounds__(128) k_sg_tc(const SurrogateDev S, const unsig
             in.features(i, S.norm, z);
             h = sg_in_hull(S.norm, z);
         }
-#pragma unroll
-        for (int k = 0; k < 16; k++) tc_store_bf16(A, t, k, k < 3 ? z[k] : 0.f);
+        {
+            const float x[8] = {z[0], z[1], z[2], 0.f, 0.f, 0.f, 0.f, 0.f}, zero[8] = {};
+            tc_store8_bf16(A, t, 0, x);
+            tc_store8_bf16(A, t, 8, zero);
+        }
         float v[64];
         // hidden layers: 3 -> 64 -> 64 -> 64, GELU
 #pragma unroll 1
         for (int L = 0; L < 3 && ok; L++) {
             const int wOff = L == 0 ? TC_W1 : (L == 1 ? TC_W2 : TC_W3);
-            const float *bias = P + (L == 0 ? SG_OFF_B1 : (L == 1 ? SG_OFF_B2 : SG_OFF_B3));
+            const float4 *bias = reinterpret_cast<const float4 *>(sm + TC_BIAS) + L * 16;
             ok = __syncthreads_and(tc_layer(sm, tmem, wOff, 64, L == 0 ? 1 : 4, phase));
             if (!ok) break;
 #pragma unroll
             for (int c = 0; c < 4; c++) tc_ld16(tw + 16 * c, v + 16 * c);
 #pragma unroll
-            for (int j = 0; j < 64; j++) tc_store_bf16(A, t, j, sg_gelu(v[j] + __ldg(bias + j)));
+            for (int j8 = 0; j8 < 8; j8++) {
+                const float4 ba = bias[2 * j8], bb = bias[2 * j8 + 1];
+                const float b8[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
+                float x[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) x[q] = sg_gelu(v[8 * j8 + q] + b8[q]);
+                tc_store8_bf16(A, t, 8 * j8, x);
+            }
         }
         if (!ok) break;
         // output layer: 64 -> 4 (N padded to 16), linear

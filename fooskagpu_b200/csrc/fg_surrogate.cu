@@ -56,9 +56,14 @@ struct Buf {
 
 constexpr int kChunks = 64;   // sample chunks of the weight-gradient reduction
 
-__device__ __forceinline__ float gelu_f(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU (tanh form) and its derivative in training: with u = c (z + a z^3), th = tanh(u),
+//   gelu = z / 2 (1 + th),  gelu' = (1 + th) / 2 + z / 2 (1 - th^2) c (1 + 3 a z^2)
+__device__ __forceinline__ float gelu_f(float z) {
+    return 0.5f * z * (1.0f + tanhf(SG_GELU_C * fmaf(SG_GELU_A * z, z * z, z)));
+}
 __device__ __forceinline__ float gelu_d(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+    const float th = tanhf(SG_GELU_C * fmaf(SG_GELU_A * z, z * z, z));
+    return 0.5f * (1.0f + th) + 0.5f * z * (1.0f - th * th) * SG_GELU_C * fmaf(3.0f * SG_GELU_A * z, z, 1.0f);
 }
 
 // rows of X and Y selected by perm[start .. start+B)

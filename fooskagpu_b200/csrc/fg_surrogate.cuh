@@ -37,7 +37,18 @@ struct SurrogateDev {
     int enabled;
 };
 
-__device__ __forceinline__ float sg_gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel, "Gaussian Error Linear Units", 2016):
+//   gelu(x) = x / 2 (1 + tanh(sqrt(2 / pi) (x + 0.044715 x^3)))
+// the network's activation in training (FP32, tanhf) and in the tensor-core inference, where the
+// hardware tanh.approx.f32 (relative error about 2^-11, below the BF16 rounding of the
+// activations that follows) keeps the epilogue short.
+constexpr float SG_GELU_C = 0.79788456080286536f, SG_GELU_A = 0.044715f;
+__device__ __forceinline__ float sg_gelu(float x) {
+    float th;
+    const float u = SG_GELU_C * fmaf(SG_GELU_A * x, x * x, x);
+    asm("tanh.approx.f32 %0, %1;" : "=f"(th) : "f"(u));
+    return 0.5f * x * (1.0f + th);
+}
 
 // Inside the training hull: per-feature box and Mahalanobis bound on the normalised inputs.
 __device__ __forceinline__ bool sg_in_hull(const SurrogateNorm &N, const float (&z)[3]) {

@@ -1,6 +1,7 @@
 """TEST INFRASTRUCTURE ONLY — FP64 numpy restatement of the equilibrium surrogate network
-(3 -> 64 -> 64 -> 64 -> 4, exact-erf GELU, mean-squared loss over the 4 outputs) with the same
-flat parameter layout as the device code, used to check the device forward / backward kernels:
+(3 -> 64 -> 64 -> 64 -> 4, GELU in its tanh form (Hendrycks & Gimpel 2016), mean-squared loss
+over the 4 outputs) with the same flat parameter layout as the device code, used to check the
+device forward / backward kernels:
 
     W1[3][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64][4] b4[4]   (W in x out)
 
@@ -10,7 +11,6 @@ inputs, FP32-like accumulation carried in FP64.
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 SIZES = [(3, 64), (64, 64), (64, 64), (64, 4)]
 NPARAM = sum(k * n + n for k, n in SIZES)
@@ -29,12 +29,17 @@ def unpack(p: np.ndarray):
     return out
 
 
+C = np.sqrt(2.0 / np.pi)
+A = 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    return 0.5 * z * (1.0 + np.tanh(C * (z + A * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    th = np.tanh(C * (z + A * z ** 3))
+    return 0.5 * (1.0 + th) + 0.5 * z * (1.0 - th * th) * C * (1.0 + 3.0 * A * z * z)
 
 
 def forward(p, X):
