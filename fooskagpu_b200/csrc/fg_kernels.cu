@@ -113,7 +113,7 @@ __device__ __forceinline__ void load_frec<float>(const float *__restrict__ FB, i
 // then each thread computes its cell's faces from shared memory only.  Strides are odd numbers
 // of words so that threads of a warp reading the same field of consecutive cells hit distinct
 // banks.  slotLocal holds the neighbour's staged-record index, or -bc on a boundary slot.
-constexpr int kGeoComp = 10;   // nx ny nz A dcx dcy dcz dnx dny dnz
+constexpr int kGeoComp = 10;   // aox aoy aoz A dcx dcy dcz dnx dny dnz
 
 template <typename T> struct Vec16;
 template <> struct Vec16<float> { using type = float4; };
@@ -149,9 +149,9 @@ struct SlotGeo {
 #else
         const size_t g = g0 + k;
         switch (comp) {
-        case 0: return m->nx[g];
-        case 1: return m->ny[g];
-        case 2: return m->nz[g];
+        case 0: return m->aox[g];
+        case 1: return m->aoy[g];
+        case 2: return m->aoz[g];
         case 3: return m->A[g];
         case 4: return m->dcx[g];
         case 5: return m->dcy[g];
@@ -193,7 +193,7 @@ __device__ __forceinline__ void stage_geometry(const DevMesh<T> &m, int lo, int 
     const size_t g0 = (size_t)lo * S;                    // 16-byte aligned: B * S * sizeof(T) % 16 == 0
     for (int i = threadIdx.x; i < kGeoComp * nV; i += blockDim.x) {
         const int cpt = i / nV, j = i % nV;
-        const V x = __ldg(reinterpret_cast<const V *>(m.nx + cpt * cstride + g0) + j);
+        const V x = __ldg(reinterpret_cast<const V *>(m.aox + cpt * cstride + g0) + j);
         reinterpret_cast<V *>(sg + (size_t)cpt * stride)[j] = x;
     }
     for (int i = threadIdx.x; i < nOwn * S; i += blockDim.x) sl[i] = m.slotLocal[g0 + i];
@@ -251,18 +251,20 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     const int nf = fl & 7;
     for (int k = 0; k < nf; k++) {
         const int li = geo.local(k);
-        const T nx = geo.get(0, k), ny = geo.get(1, k), nz = geo.get(2, k), A = geo.get(3, k);
-        const T sgn = ((fl >> (3 + k)) & 1) ? (T)1 : (T)-1;   // outward orientation of this cell
+        // outward n A of the face (the host computed (+-1) n A in T arithmetic, as the reference's
+        // sign times normal times area)
+        const T ax = geo.get(0, k), ay = geo.get(1, k), az = geo.get(2, k);
         T ot[NP];
         if (li >= 0) {
 #pragma unroll
             for (int v = 0; v < NP; v++) ot[v] = rec[li * WS + v];
         } else {
+            // boundary slot: the cell owns the face, so its canonical normal points outward
+            const int fi = m.slotFace[(size_t)c * m.nSlots + k];
 #pragma unroll
             for (int v = 0; v < NP; v++) ot[v] = w[v];
-            ghost_state(P, -li, nx, ny, nz, ot);
+            ghost_state(P, -li, m.fnx[fi], m.fny[fi], m.fnz[fi], ot);
         }
-        const T ax = sgn * nx * A, ay = sgn * ny * A, az = sgn * nz * A;
 #pragma unroll
         for (int v = 0; v < NP; v++) {
             mx[v] = fmax(mx[v], ot[v]);

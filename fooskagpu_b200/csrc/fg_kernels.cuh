@@ -17,7 +17,8 @@ struct DevMesh {
     // order, starting at nx; geoStride >= n * nSlots is a multiple of 16 bytes so that every
     // component starts 16-byte aligned and 16-byte reads of a block's range stay inside it
     size_t geoStride;
-    const T *nx, *ny, *nz, *A;       // canonical (owner -> neighbour) unit normal and area
+    const T *aox, *aoy, *aoz;        // outward area vector of the slot's face seen from the cell, n A
+    const T *A;                      // face area
     const T *dcx, *dcy, *dcz;        // face centre - own cell centre
     const T *dnx, *dny, *dnz;        // face centre - neighbour cell centre (periodic image)
     const double *vol;               // cell volume

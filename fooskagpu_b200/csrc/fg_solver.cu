@@ -373,7 +373,9 @@ struct SolverT : public fg_solver {
                 } else {
                     nbr[q] = m.old2new[own];
                 }
-                for (int d = 0; d < 3; d++) geo[(size_t)d * GS + q] = (T)m.n[(size_t)f * 3 + d];
+                // outward n A in T arithmetic: (+-1) * n * A, the gradient's operand order
+                const T sg = (side == 0) ? (T)1 : (T)-1;
+                for (int d = 0; d < 3; d++) geo[(size_t)d * GS + q] = sg * (T)m.n[(size_t)f * 3 + d] * (T)m.area[f];
                 geo[3 * GS + q] = (T)m.area[f];
                 for (int d = 0; d < 3; d++) {
                     const double dcv = (side == 0) ? xOwnSide[d] - m.cellCenter[(size_t)o * 3 + d]
@@ -555,7 +557,7 @@ struct SolverT : public fg_solver {
         dm.flags = dFlags.as<int32_t>();
         T *g = dGeo.as<T>();
         dm.geoStride = GS;
-        dm.nx = g + 0 * GS; dm.ny = g + 1 * GS; dm.nz = g + 2 * GS; dm.A = g + 3 * GS;
+        dm.aox = g + 0 * GS; dm.aoy = g + 1 * GS; dm.aoz = g + 2 * GS; dm.A = g + 3 * GS;
         dm.dcx = g + 4 * GS; dm.dcy = g + 5 * GS; dm.dcz = g + 6 * GS;
         dm.dnx = g + 7 * GS; dm.dny = g + 8 * GS; dm.dnz = g + 9 * GS;
         dm.vol = dVol.as<double>();

@@ -7,7 +7,7 @@ whole-mesh run's bit for bit, in both precisions, for 2 and 3 parts."""
 import numpy as np
 import pytest
 
-from gpu_cases import make
+from gpu_cases import TIE_TOL, make
 from halo_threads import ThreadGroup, ThreadHalo, run_parts
 from fooskagpu_b200.api import Solver
 
@@ -53,6 +53,65 @@ def test_partitioned_matches_whole_mesh(name, P, prec, meshdir):
         assert halos[p].exchanges == 2 * c.rkSteps * STEPS
     for s in solvers:
         s.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_partitioned_with_surrogate_matches_whole_mesh(prec, meshdir):
+    """The chemical relaxation with the learned surrogate: each part runs the tensor-core
+    pre-pass over its own chemical cells; per cell the prediction and the polish are those of
+    the whole-mesh run."""
+    from fooskagpu_b200 import cases, meshgen
+    from fooskagpu_b200.api import Mesh, Surrogate
+    path = str(meshdir / "part_sg_box.neu")
+    meshgen.write_neu(path, meshgen.box_tets(20, 10, 10, L=(0.02, 0.01, 0.01), jitter=0.1,
+                                             side_bc={k: "slip" for k in ("x0", "x1", "y0", "y1", "z0", "z1")}))
+    m = Mesh.load_neu(path, scale=1.0)
+    c = cases.reference_case()
+    c.rkSteps = 3
+    c.hllcTieTol = TIE_TOL[prec]
+    U = cases.perturbed_two_phase_ic(c, m.arrays()["cellCenter"], seed=8, vel=25.0)
+    s = Solver(m, c, precision="fp64")
+    s.set_state(U)
+    s.relax_log(1_000_000)
+    for _ in range(3):
+        s.step()
+    X, Y = s.relax_log_read(1_000_000)
+    s.close()
+    g = Surrogate(seed=4)
+    g.set_data(X, Y)
+    g.train(10, batch=256, lr=2e-3, seed=5)
+    s = Solver(m, c, precision=prec)
+    s.set_state(U)
+    s.set_surrogate(g, 1e-6, 3)
+    for _ in range(STEPS):
+        s.step()
+    Uw = s.get_state()
+    sw = s.relax_stats()
+    s.close()
+    P = 2
+    parts = [m.partition(P, p) for p in range(P)]
+    group = ThreadGroup(P)
+    solvers = [Solver(pm, c, precision=prec) for pm in parts]
+    halos = [ThreadHalo(group, sp, pm) for sp, pm in zip(solvers, parts)]
+    own = [pm.partition_maps()["cell_global"][:pm.n_owned] for pm in parts]
+    for sp, cg in zip(solvers, own):
+        sp.set_state(U[cg])
+        sp.set_surrogate(g, 1e-6, 3)
+
+    def run(p):
+        for _ in range(STEPS):
+            solvers[p].step()
+        return solvers[p].get_state(), solvers[p].relax_stats()
+
+    res = run_parts(run, group)
+    assert sw["nSurrogate"] > 0
+    assert sum(r[1]["nSurrogate"] for r in res) == sw["nSurrogate"]
+    assert sum(r[1]["nChem"] for r in res) == sw["nChem"]
+    for p in range(P):
+        assert np.array_equal(res[p][0], Uw[own[p]]), (p, np.abs(res[p][0] - Uw[own[p]]).max())
+    for sp in solvers:
+        sp.close()
+    g.close()
 
 
 def test_part_solver_needs_a_transport(meshdir):
