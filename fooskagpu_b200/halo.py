@@ -44,6 +44,10 @@ class TorchHalo:
         self.send = torch.empty(max(sb, 16), dtype=torch.uint8, device=self.device)
         self.recv = torch.empty(max(rb, 16), dtype=torch.uint8, device=self.device)
         self.exchanges = 0
+        # one collective of the whole group before the first batched point-to-point call: NCCL
+        # lets later batches involve only the neighbouring ranks after that (a part need not
+        # touch every other part)
+        self._allreduce(L.FG_REDUCE_SUM, 0.0)
         solver.set_halo(self._exchange, self._allreduce, self.send.data_ptr(), self.recv.data_ptr())
 
     def _sync(self):

@@ -1,5 +1,5 @@
-"""The torch.distributed transport of a partitioned run (fooskagpu_b200.halo.TorchHalo) with 2 and
-3 gloo ranks on the CPU: every rank packs the records of its send cells, one exchange later each
+"""The torch.distributed transport of a partitioned run (fooskagpu_b200.halo.TorchHalo) with 2, 3
+and 4 gloo ranks on the CPU (with 4, some parts have no face in common): every rank packs the records of its send cells, one exchange later each
 rank holds exactly its ghosts' records (both record sizes of the mixed and FP64 paths), and the
 dt / conservation reductions give the minimum / sum over the ranks.  The solver is replaced by a
 stand-in that only owns the buffers (the kernels that pack and unpack them run on the GPU)."""
@@ -67,7 +67,7 @@ def _rank(rank, world, port, path, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 4])
 def test_gloo_halo_exchange(world, tmp_path):
     sys.path.insert(0, str(ROOT))
     from fooskagpu_b200 import meshgen
