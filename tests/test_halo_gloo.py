@@ -72,7 +72,9 @@ def test_gloo_halo_exchange(world, tmp_path):
     sys.path.insert(0, str(ROOT))
     from fooskagpu_b200 import meshgen
     path = str(tmp_path / "halo.neu")
-    meshgen.write_neu(path, meshgen.box_tets(8, 4, 3, L=(0.8, 0.4, 0.3), jitter=0.1, shuffle=True,
+    # 16 x 4 x 4 cells in 4 parts: parts 0 and 3 (and 1 and 2) share no face
+    shape = (8, 4, 3) if world < 4 else (16, 4, 4)
+    meshgen.write_neu(path, meshgen.box_tets(*shape, L=tuple(0.1 * k for k in shape), jitter=0.1, shuffle=True,
                                              side_bc={s: "slip" for s in ("x0", "x1", "y0", "y1", "z0", "z1")}))
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
