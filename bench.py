@@ -411,7 +411,8 @@ def reference_gpu(args):
     the reference sources by oracle/build_ref.py) on the nearest workload it can express: the
     same 128^3 hex cube, TGV state and case, with slip walls in place of the periodic faces
     (the reference has no periodic boundary), elements in the same shuffled order (the reference
-    does not renumber).  Timed by the driver's CUDA events around the step loop."""
+    does not renumber).  Timed by CUDA events that oracle/ref_driver.cu records around its step
+    loop."""
     from oracle import ref_run
     if not ref_run.available():
         return {"unavailable": "reference GPU build oracle/_ref/fooska_ref_dp not present (built from the reference sources)"}

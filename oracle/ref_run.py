@@ -41,8 +41,8 @@ def write_case_file(path, c) -> None:
 
 def run(workdir, neu_path, case, U, steps: int, warmup: int = 0, dump: bool = False, timeout: float = 300.0) -> dict:
     """Run `steps` explicitLoop iterations (after `warmup` untimed ones) of the reference solver
-    on mesh `neu_path` from state U (nElem x 10, .neu element order).  Returns the driver's
-    report: cells, steps, ms (CUDA events over the timed steps), physical time, dt, status."""
+    on mesh `neu_path` from state U (nElem x 10, .neu element order).  Returns the report of
+    oracle/ref_driver.cu: cells, steps, ms (CUDA events over the timed steps), physical time, dt, status."""
     wd = Path(workdir).resolve()
     wd.mkdir(parents=True, exist_ok=True)
     sh = wd / "sh.neu"

@@ -7,8 +7,8 @@
   oracle/build_ref.py).  Needs the reference tree; run here, commit the .npz.
 
 * ``stage_*.npz`` — stage-level fixtures produced by the reference CUDA binary
-  (oracle/_ref/fooska_ref_dp) on a B200, see ``run_stage_fixtures`` (invoked on the GPU box,
-  files land in gpurun_out/ and are copied here).
+  (oracle/_ref/fooska_ref_dp) on a B200, see ``run_stage_fixtures`` (run on a machine with the
+  GPU into <outdir>, then packed here by ``collect``).
 
 usage: python tests/golden/make_golden.py kat
        python tests/golden/make_golden.py stage <outdir>     (GPU box)
