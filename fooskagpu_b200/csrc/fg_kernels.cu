@@ -113,7 +113,7 @@ __device__ __forceinline__ void load_frec<float>(const float *__restrict__ FB, i
 // then each thread computes its cell's faces from shared memory only.  Strides are odd numbers
 // of words so that threads of a warp reading the same field of consecutive cells hit distinct
 // banks.  slotLocal holds the neighbour's staged-record index, or -bc on a boundary slot.
-constexpr int kGeoComp = 10;   // aox aoy aoz A dcx dcy dcz dnx dny dnz
+constexpr int kGeoComp = 6;    // aox aoy aoz dcx dcy dcz
 
 template <typename T> struct Vec16;
 template <> struct Vec16<float> { using type = float4; };
@@ -152,13 +152,9 @@ struct SlotGeo {
         case 0: return m->aox[g];
         case 1: return m->aoy[g];
         case 2: return m->aoz[g];
-        case 3: return m->A[g];
-        case 4: return m->dcx[g];
-        case 5: return m->dcy[g];
-        case 6: return m->dcz[g];
-        case 7: return m->dnx[g];
-        case 8: return m->dny[g];
-        default: return m->dnz[g];
+        case 3: return m->dcx[g];
+        case 4: return m->dcy[g];
+        default: return m->dcz[g];
         }
 #endif
     }
@@ -283,7 +279,7 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
 #pragma unroll
     for (int v = 0; v < NP; v++) th[v] = (T)1e9;
     for (int k = 0; k < nf; k++) {
-        const T dx = geo.get(4, k), dy = geo.get(5, k), dz = geo.get(6, k);
+        const T dx = geo.get(3, k), dy = geo.get(4, k), dz = geo.get(5, k);
 #pragma unroll
         for (int v = 0; v < NP; v++) {
             const T ext = dx * gs[3 * v] + dy * gs[3 * v + 1] + dz * gs[3 * v + 2];

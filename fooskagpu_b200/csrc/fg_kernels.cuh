@@ -13,14 +13,12 @@ struct DevMesh {
     int nSlots;         // max faces per cell
     const int32_t *nbr;   // neighbour cell, or -bc (1..5) on a boundary slot, or INT32_MIN unused
     const int32_t *flags; // bits 0-2: faces of the cell; bit 3+k: cell owns the face of slot k
-    // the ten per-slot geometry arrays below are consecutive blocks of geoStride values, in this
-    // order, starting at nx; geoStride >= n * nSlots is a multiple of 16 bytes so that every
+    // the six per-slot geometry arrays below are consecutive blocks of geoStride values, in this
+    // order, starting at aox; geoStride >= n * nSlots is a multiple of 16 bytes so that every
     // component starts 16-byte aligned and 16-byte reads of a block's range stay inside it
     size_t geoStride;
     const T *aox, *aoy, *aoz;        // outward area vector of the slot's face seen from the cell, n A
-    const T *A;                      // face area
     const T *dcx, *dcy, *dcz;        // face centre - own cell centre
-    const T *dnx, *dny, *dnz;        // face centre - neighbour cell centre (periodic image)
     const double *vol;               // cell volume
     const double *volP;              // pow(vol, 0.3333) as the reference's CFL bound uses
     // shared-memory staging: blocks of `blockCells` consecutive cells; the face neighbours of a

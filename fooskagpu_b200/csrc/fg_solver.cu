@@ -344,7 +344,7 @@ struct SolverT : public fg_solver {
         // component stride of the geometry arrays: padded to 16 bytes (see DevMesh::geoStride)
         const size_t GS = (S * sizeof(T) + 15) / 16 * 16 / sizeof(T);
         std::vector<int32_t> nbr(S, INT32_MIN), flags(n, 0);
-        std::vector<T> geo(10 * GS, (T)0);
+        std::vector<T> geo(6 * GS, (T)0);
         std::vector<double> volP(n), vol(n);
         for (int i = 0; i < n; i++) {
             const int o = m.new2old[i];
@@ -376,15 +376,11 @@ struct SolverT : public fg_solver {
                 // outward n A in T arithmetic: (+-1) * n * A, the gradient's operand order
                 const T sg = (side == 0) ? (T)1 : (T)-1;
                 for (int d = 0; d < 3; d++) geo[(size_t)d * GS + q] = sg * (T)m.n[(size_t)f * 3 + d] * (T)m.area[f];
-                geo[3 * GS + q] = (T)m.area[f];
+                // face centre (the periodic image on the neighbour's side) - own cell centre
                 for (int d = 0; d < 3; d++) {
                     const double dcv = (side == 0) ? xOwnSide[d] - m.cellCenter[(size_t)o * 3 + d]
                                                    : xNbSide[d] - m.cellCenter[(size_t)o * 3 + d];
-                    double dnv = 0.0;
-                    if (side == 0 && bc == 0) dnv = xNbSide[d] - m.cellCenter[(size_t)nbo * 3 + d];
-                    if (side == 1) dnv = xOwnSide[d] - m.cellCenter[(size_t)own * 3 + d];
-                    geo[(size_t)(4 + d) * GS + q] = (T)dcv;
-                    geo[(size_t)(7 + d) * GS + q] = (T)dnv;
+                    geo[(size_t)(3 + d) * GS + q] = (T)dcv;
                 }
             }
             flags[i] = fl;
@@ -494,13 +490,13 @@ struct SolverT : public fg_solver {
         dm.slotLocal = dSlotLocal.as<int16_t>();
         FG_CUDA_TRY(dNbr.alloc(S * sizeof(int32_t)));
         FG_CUDA_TRY(dFlags.alloc((size_t)n * sizeof(int32_t)));
-        FG_CUDA_TRY(dGeo.alloc(10 * GS * sizeof(T)));
+        FG_CUDA_TRY(dGeo.alloc(6 * GS * sizeof(T)));
         FG_CUDA_TRY(dVol.alloc((size_t)n * sizeof(double)));
         FG_CUDA_TRY(dVolP.alloc((size_t)n * sizeof(double)));
         FG_CUDA_TRY(dNew2Old.alloc((size_t)n * sizeof(int32_t)));
         FG_CUDA_TRY(cudaMemcpy(dNbr.p, nbr.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dFlags.p, flags.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
-        FG_CUDA_TRY(cudaMemcpy(dGeo.p, geo.data(), 10 * GS * sizeof(T), cudaMemcpyHostToDevice));
+        FG_CUDA_TRY(cudaMemcpy(dGeo.p, geo.data(), 6 * GS * sizeof(T), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dVol.p, vol.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dVolP.p, volP.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
         FG_CUDA_TRY(cudaMemcpy(dNew2Old.p, m.new2old.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
@@ -557,9 +553,8 @@ struct SolverT : public fg_solver {
         dm.flags = dFlags.as<int32_t>();
         T *g = dGeo.as<T>();
         dm.geoStride = GS;
-        dm.aox = g + 0 * GS; dm.aoy = g + 1 * GS; dm.aoz = g + 2 * GS; dm.A = g + 3 * GS;
-        dm.dcx = g + 4 * GS; dm.dcy = g + 5 * GS; dm.dcz = g + 6 * GS;
-        dm.dnx = g + 7 * GS; dm.dny = g + 8 * GS; dm.dnz = g + 9 * GS;
+        dm.aox = g + 0 * GS; dm.aoy = g + 1 * GS; dm.aoz = g + 2 * GS;
+        dm.dcx = g + 3 * GS; dm.dcy = g + 4 * GS; dm.dcz = g + 5 * GS;
         dm.vol = dVol.as<double>();
         dm.volP = dVolP.as<double>();
         dm.nF = nF;
