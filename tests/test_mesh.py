@@ -112,3 +112,28 @@ def test_renumbering_is_a_permutation(tmp_path):
         assert np.array_equal(np.sort(perm), np.arange(m.n_elem))
         if r == "none":
             assert np.array_equal(perm, np.arange(m.n_elem))
+
+
+def test_smallest_meshes(tmp_path):
+    """Edge sizes: a file with no elements is rejected; one cell (six boundary faces) loads and
+    partitions only into one part."""
+    p = str(tmp_path / "one.neu")
+    meshgen.write_neu(p, meshgen.box_hexes(1, 1, 1, side_bc=SLIP))
+    m = Mesh.load_neu(p)
+    assert m.n_elem == 1 and m.n_fcs == 6 and m.info["nBoundary"] == 6
+    assert m.partition(1, 0).n_elem == 1
+    with pytest.raises(FgError, match="nParts"):
+        m.partition(2, 0)
+    lines = open(p).read().split("\n")
+    i = next(k for k, l in enumerate(lines) if l.strip().startswith("NUMNP"))
+    hdr = lines[i + 1].split()
+    hdr[1] = "0"
+    lines[i + 1] = " ".join(hdr)
+    txt = "\n".join(lines)
+    a = txt.index("ELEMENTS/CELLS")
+    b = txt.index("ENDOFSECTION", a)
+    q = str(tmp_path / "zero.neu")
+    open(q, "w").write(txt[:a] + txt[a:].split("\n", 1)[0] + "\n" + txt[b:])
+    with pytest.raises(FgError) as e:
+        Mesh.load_neu(q)
+    assert e.value.code == 3
