@@ -360,6 +360,22 @@ class Surrogate:
         v = np.ascontiguousarray(v, dtype=np.float32)
         check(lib().fg_surrogate_set_norm(self._h, _fptr(v)))
 
+    def save(self, path: str) -> None:
+        """The trained network (FP32 parameters and the input / output normalisation) as .npz."""
+        np.savez(path, params=self.params(), norm=self.norm(), layout=np.array([self.NPARAM, self.NNORM]))
+
+    @classmethod
+    def load(cls, path: str, device: int = 0) -> "Surrogate":
+        """A surrogate with the parameters and normalisation saved by `save` (ready to predict
+        and to attach to a solver; set_data is needed only to train further)."""
+        d = np.load(path)
+        if list(d["layout"]) != [cls.NPARAM, cls.NNORM]:
+            raise ValueError(f"{path}: network layout {list(d['layout'])} differs from {[cls.NPARAM, cls.NNORM]}")
+        g = cls(device=device)
+        g.set_params(d["params"])
+        g.set_norm(d["norm"])
+        return g
+
     def predict(self, X: np.ndarray):
         """Tensor-core forward of raw inputs: (outputs [n][4], in-hull flags [n])."""
         X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, 3)

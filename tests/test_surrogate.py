@@ -204,3 +204,28 @@ def test_mixed_surrogate_steps_vs_fp64_newton(box, trained):
     e_p = float(np.linalg.norm(pa - pb) / np.linalg.norm(pb))
     _report("surrogate/steps", dict(rho_l2=e_rho, p_l2=e_p))
     assert e_rho < 1e-3 and e_p < 1e-3, (e_rho, e_p)
+
+
+def test_save_and_load(box, trained, data, tmp_path):
+    """A trained network saved to .npz and loaded into a new surrogate predicts the same outputs
+    bit for bit, and relaxes a state to the same result."""
+    m, c, cc = box
+    g = trained[0]
+    X, _ = data
+    path = str(tmp_path / "sg.npz")
+    g.save(path)
+    h = Surrogate.load(path)
+    P0, h0 = g.predict(X[:2048])
+    P1, h1 = h.predict(X[:2048])
+    assert np.array_equal(P0, P1) and np.array_equal(h0, h1)
+    U = cases.perturbed_two_phase_ic(c, cc, seed=13, vel=25.0)
+    out = []
+    for sg in (g, h):
+        s = Solver(m, c, precision="fp64")
+        s.set_state(U)
+        s.set_surrogate(sg, REL_TOL, POLISH)
+        s.relaxation()
+        out.append(s.get_state())
+        s.close()
+    assert np.array_equal(out[0], out[1])
+    h.close()
