@@ -123,3 +123,14 @@ def test_part_solver_needs_a_transport(meshdir):
     with pytest.raises(FgError, match="fg_solver_set_halo"):
         s.step()
     s.close()
+
+
+def test_transport_only_for_parts(meshdir):
+    """A solver of a whole mesh has no halo: no buffers, and a transport is refused."""
+    from fooskagpu_b200._lib import FgError
+    m, c, U = make("tet_ref", meshdir, "fp64")
+    s = Solver(m, c, precision="fp64")
+    assert s.halo_buffer_bytes() == (0, 0)
+    with pytest.raises(FgError, match="not a part"):
+        s.set_halo(lambda f, rb, st: None, lambda op, v: v, 0, 0)
+    s.close()
