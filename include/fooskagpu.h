@@ -246,7 +246,10 @@ int fg_halo_buffer_bytes(const fg_solver *s, int64_t *sendBytes, int64_t *recvBy
 int fg_solver_set_halo(fg_solver *s, const fg_halo_ops *ops, void *sendBuf, void *recvBuf);
 
 /* Replaces initialize / readField (DP/initialize.cu:61, DP/restart.cu:424): upload U
- * (nElem*10 doubles, reference order) from host memory.  stream may be NULL. */
+ * (nElem*10 doubles, reference order; the own cells of a part mesh) from host memory.  The
+ * upload is checked on the device before it replaces the state: FG_ERR_NAN names the first cell
+ * that is not finite, has alpha outside [0, 1] or a negative partial density, and the state is
+ * left as it was.  Synchronises `stream` (may be NULL). */
 int fg_set_state(fg_solver *s, const double *U, void *stream);
 /* Download U (nElem*10 doubles, reference order).  Synchronises `stream`. */
 int fg_get_state(fg_solver *s, double *U, void *stream);
