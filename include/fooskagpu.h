@@ -336,12 +336,16 @@ int fg_cons_calc(fg_solver *s, int32_t ivar, double *out, void *stream);
  * pool allocator owns all device memory, a monitor between the steps of a latency-critical
  * loop where cudaMalloc / cudaFree may synchronise the device).
  * U: device, reference layout U[cell*10 + v]; vol: device, nCells volumes; out: device, one
- * double, receives the integral of variable ivar (ivar 0 integrates 1-alpha), as fg_cons_calc.
+ * double, receives the integral of variable ivar (ivar 0 integrates 1-alpha).  The result is
+ * deterministic for a given nCells and cell order; it agrees with fg_cons_calc (which sums the
+ * cells in the solver's own device order) to rounding, not bit for bit.
  * Runs on the calling thread's current device, asynchronously on `stream`.
  * The block partial sums go to a static device array of FG_NOALLOC_MAX_CELLS/256 doubles
  * (512 KiB, held on every device that loads the library until exit); nCells above
  * FG_NOALLOC_MAX_CELLS is rejected with FG_ERR_ARG.  The first call on a device looks the
- * array's address up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * array's address up (cudaGetSymbolAddress) and keeps it for the life of the process: make that
+ * first call before any stream capture, and do not call it on a device that was reset
+ * (cudaDeviceReset) after its first call there.
  * All calls on a device share the array: calls that overlap on the GPU race. */
 #define FG_NOALLOC_MAX_CELLS (65536 * 256)
 int fg_cons_integral_noalloc(const double *U, const double *vol, int32_t nCells, int32_t ivar, double *out,

@@ -10,7 +10,7 @@ solver from its own sources (read in place under the reference tree) into oracle
 
 Nothing from the reference is copied into the repository: sources are compiled where they
 lie and the outputs stay in oracle/_ref/ (git-ignored).  Usage:
-    python oracle/build_ref.py [--ref /path/to/reference]
+    python oracle/build_ref.py --ref <reference tree>      (or set FOOSKA_REFERENCE)
 """
 from __future__ import annotations
 
@@ -23,7 +23,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 SHIM = HERE / "refshim"
-DEFAULT_REF = Path("/root/reference")
+# the reference tree: --ref, or the FOOSKA_REFERENCE environment variable (no default)
+DEFAULT_REF = Path(os.environ["FOOSKA_REFERENCE"]) if os.environ.get("FOOSKA_REFERENCE") else None
 DP_SUB = "mulitphase Solver/doublePrecision"
 
 # reference translation units linked into the GPU binary (the driver replaces the others)
@@ -45,7 +46,7 @@ def dp_dir(ref: Path) -> Path:
 
 
 def available(ref: Path = DEFAULT_REF) -> bool:
-    return (dp_dir(ref) / "eqos.h").exists()
+    return ref is not None and (dp_dir(Path(ref)) / "eqos.h").exists()
 
 
 def build_host(ref: Path = DEFAULT_REF, force: bool = False) -> Path:
@@ -99,14 +100,15 @@ def build_gpu(ref: Path = DEFAULT_REF, force: bool = False) -> Path:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=str(DEFAULT_REF))
+    ap.add_argument("--ref", default=str(DEFAULT_REF) if DEFAULT_REF else None,
+                    help="reference tree (default: the FOOSKA_REFERENCE environment variable)")
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--host-only", action="store_true")
     a = ap.parse_args()
-    ref = Path(a.ref)
-    if not available(ref):
-        print("reference tree not found; nothing to build")
+    if not a.ref or not available(Path(a.ref)):
+        print("reference tree not found (give --ref or set FOOSKA_REFERENCE); nothing to build")
         return
+    ref = Path(a.ref)
     print(build_host(ref, a.force))
     if not a.host_only:
         print(build_gpu(ref, a.force))
