@@ -74,6 +74,19 @@ def mesh_setup_times(path: str, per) -> dict:
     return out
 
 
+# the time step (with its signal-speed residual) and the conservation integral every 20 steps
+# (the reference's default is 100): a timed window of 20 steps holds exactly one such step, so
+# their cost is inside the number in its natural proportion
+TGV_DT_EVERY = 20
+
+
+def bench_tgv_case(base=None):
+    from fooskagpu_b200 import cases
+    c = cases.tgv_case(base=base)
+    c.adaptDtItr = TGV_DT_EVERY
+    return c
+
+
 def tgv_mesh(rank: int, world: int, dist):
     from fooskagpu_b200 import meshgen
     L = 2 * math.pi
@@ -174,7 +187,7 @@ def run_ours(args, rank, world, local_rank, dist):
     mesh = Mesh.load_neu(path, scale=1.0, periodic=per, gpu=True, device=dev)
     nE = mesh.n_elem
     info = mesh.info
-    case = cases.tgv_case()
+    case = bench_tgv_case()
     a = mesh.arrays()
     U0 = cases.tgv_ic(case, a["cellCenter"])
     del a
@@ -211,26 +224,44 @@ def run_ours(args, rank, world, local_rank, dist):
     prof = s.profile_read()
     s.profile(False)
     mem = s.memory_bytes()
-    # end to end through the C ABI with pinned host buffers
-    Uh = torch.empty((nE, 10), dtype=torch.float64, pin_memory=True)
-    Uh.numpy()[:] = U0
+    # end to end through the C ABI with pinned host buffers: every step uploads the state
+    # (fg_set_state_async: copy, device check, scatter; no host round trip), steps, and reads the
+    # state back (fg_get_state: gather, copy, synchronise)
+    Uin = torch.empty((nE, 10), dtype=torch.float64, pin_memory=True)
+    Uin.numpy()[:] = U0
+    Uout = torch.empty((nE, 10), dtype=torch.float64, pin_memory=True)
     e2e_steps = max(3, min(args.steps, 20))
-    s.set_state(Uh.numpy(), stream=stream.cuda_stream)
+    s.set_state_async(Uin.numpy(), stream=stream.cuda_stream)
     s.step(stream=stream.cuda_stream)
-    s.get_state(Uh.numpy(), stream=stream.cuda_stream)
+    s.get_state(Uout.numpy(), stream=stream.cuda_stream)
     barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e2e_steps):
-        s.set_state(Uh.numpy(), stream=stream.cuda_stream)
+        s.set_state_async(Uin.numpy(), stream=stream.cuda_stream)
         s.step(stream=stream.cuda_stream)
-        s.get_state(Uh.numpy(), stream=stream.cuda_stream)
+        s.get_state(Uout.numpy(), stream=stream.cuda_stream)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e_val = job_value(world, nE, rk, e2e_steps, e2e_ms)
+    s.check_state()
+    # the copies alone: upload (+ check + scatter) and download (+ gather) bandwidths
+    def copy_gbs(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(reps):
+            fn()
+        c1.record(stream)
+        torch.cuda.synchronize()
+        return nE * 80 * reps / (c0.elapsed_time(c1) / 1e3) / 1e9
+    h2d_gbs = copy_gbs(lambda: s.set_state_async(Uin.numpy(), stream=stream.cuda_stream))
+    d2h_gbs = copy_gbs(lambda: s.get_state(Uout.numpy(), stream=stream.cuda_stream))
     s.close()
 
     # ---------------- FP64 path on the same workload
@@ -276,10 +307,12 @@ def run_ours(args, rank, world, local_rank, dist):
                 "rk_stages": rk, "mesh_format": "gambit .neu, elements shuffled (seed 20261203), Morton renumbered",
                 "parallelism": "replicas" if world > 1 else "single-gpu",
                 "l2": f"inputs larger than L2 (device working set {mem / 1e9:.2f} GB)",
-                "dt": "adaptive every 100 steps (CFL 0.5)"},
+                "dt": f"adaptive every {TGV_DT_EVERY} steps (CFL 0.5): the timed steps include the dt and "
+                      "conservation steps in proportion"},
         fp64_value=fp64_value, mixed_over_fp64=value / fp64_value,
         e2e={"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nE * 80, "d2h_bytes_per_step": nE * 80,
-             "steps": e2e_steps},
+             "steps": e2e_steps, "h2d_gbs": h2d_gbs, "d2h_gbs": d2h_gbs,
+             "api": "fg_set_state_async + fg_step + fg_get_state, pinned host buffers, one stream"},
         gpu_launches=launches,
         roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                   "traffic": traffic, "kernel": "k_face<float> + k_gather<float> (face flux, owner-side gather + RK)",
@@ -293,36 +326,50 @@ def run_ours(args, rank, world, local_rank, dist):
     # ---------------- mesh pre-processing, host vs GPU (rank 0)
     if rank == 0 and not args.no_mesh_timing:
         out["mesh_preprocess"] = mesh_setup_times(path, per)
-    # ---------------- two-phase workload with the Gibbs relaxation and the learned surrogate
+    # ---------------- two-phase bubble collapse with the Gibbs relaxation and the learned surrogate
     if not args.no_two_phase:
-        out["two_phase"] = two_phase(args, torch, stream, dev)
-    # ---------------- CPU baseline (rank 0, N = 1 only): oracle FP64 on the host cores
+        out["two_phase"] = bubble(args, torch, stream, dev)
+    # ---------------- CPU baseline (rank 0, N = 1 only): oracle FP64 on the host cores; its final
+    # state is the reference of the accuracy check of both GPU paths
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(mesh, case, U0, max_stages=args.cpu_stages)
+        out["cpu_baseline"], Uref = cpu_baseline(mesh.view(), case, U0, steps=args.cpu_steps)
+        out["accuracy"] = accuracy(mesh, case, U0, Uref, args.cpu_steps, dev, torch, stream)
     return out
 
 
-def two_phase(args, torch, stream, dev):
-    """Two-phase workload with the chemical (Gibbs) relaxation active: the reference's own fluid
-    constants (DP/buildInput.cu) on a cube of NTP^3 hexes with slip walls and a smoothly
-    perturbed liquid/vapour state (about half of the cells need the Gibbs solve each step).
-    FP64 Newton-only vs mixed precision with and without the learned surrogate; the surrogate is
-    trained inside this run on samples logged from the FP64 run's first steps."""
+def bubble(args, torch, stream, dev):
+    """Two-phase water / vapour Rayleigh bubble collapse (the bubble-collapse configurations):
+    a ball of radius 10 R0 = 10 mm, about 4 M tets graded toward the centre (meshgen.ball_tets,
+    built in memory with the GPU pre-processor), a vapour bubble of R0 = 1 mm at 2340 Pa in water at
+    10 MPa (Rayleigh-Plesset pressure field, 298.15 K), stiffened-gas water / vapour constants
+    (cases.water_vapour_constants), Gibbs-equilibrium Newton relaxation, HLLC + MUSCL with the van
+    Albada-type limiter, SSP-RK3.  Three runs of the same `steps` steps from the same state:
+      - FP64 with the reference Newton, logging the converged chemical solves (training data);
+      - mixed precision with the Newton;
+      - mixed precision with the learned surrogate, trained here on the logged states.
+    Every step is timed by CUDA events; between steps (outside the timed regions) fg_probe gives
+    the vapour volume and the pressure extrema.  The collapse time is the first time the vapour
+    volume falls below 10 % of its initial value (linear between steps); the peak pressure is the
+    largest mixture pressure seen up to then."""
     from fooskagpu_b200 import cases, meshgen
     from fooskagpu_b200.api import Mesh, Solver, Surrogate
-    ntp = int(os.environ.get("FG_BENCH_TP_N", "96"))
-    MESH_DIR.mkdir(parents=True, exist_ok=True)
-    path = MESH_DIR / f"two_phase_box{ntp}.neu"
-    if not path.exists():
-        meshgen.write_neu(str(path), meshgen.box_hexes(ntp, ntp, ntp, L=(0.02, 0.02, 0.02)))
-    mesh = Mesh.load_neu(str(path), scale=1.0)
-    case = cases.reference_case()
-    case.rkSteps = 3
-    case.hllcTieTol = 1e-4
-    U0 = cases.perturbed_two_phase_ic(case, mesh.arrays()["cellCenter"], seed=5, vel=25.0)
+    n = int(os.environ.get("FG_BENCH_BALL_N", "91"))
+    steps = int(os.environ.get("FG_BENCH_BALL_STEPS", "1000"))
+    t0 = time.perf_counter()
+    nm = meshgen.ball_tets(n)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    mesh = Mesh.build(nm.nodes, nm.elems, nm.bcs, gpu=True, device=dev)
+    pre_s = time.perf_counter() - t0
+    del nm
+    case = cases.water_vapour_case()
+    U0 = cases.bubble_ic(case, mesh.arrays()["cellCenter"], width=1.5 * meshgen.ball_spacing(n, 1e-3))
     nE = mesh.n_elem
-    steps, warm = max(5, min(args.steps, 20)), 3
-    res = {"workload": f"two_phase_reference_fluid_{ntp}^3_hex_slip", "cells": nE, "steps": steps, "warmup": warm}
+    res = {"workload": f"bubble_collapse_water_vapour_ball_{nE}_tets", "cells": nE, "faces": mesh.n_fcs,
+           "steps": steps, "mesh": {"generator": f"meshgen.ball_tets({n})", "generate_s": gen_s,
+                                    "gpu_preprocess_s": pre_s}}
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
 
     def run(prec, sg=None, log=0):
         s = Solver(mesh, case, precision=prec, device=dev)
@@ -331,79 +378,162 @@ def two_phase(args, torch, stream, dev):
             s.relax_log(log)
         if sg is not None:
             s.set_surrogate(sg, 1e-6, 3)
-        for _ in range(warm):
-            s.step(stream=stream.cuda_stream)
-        data = s.relax_log_read(log) if log else None
-        if log:
-            s.relax_log(0)
-        ms = time_steps(s, steps, torch, stream)
-        st = s.relax_stats()                           # the last timed step's relaxation
+        v0 = s.probe()["vapourVolume"]
+        hist, ms, tc, pk, failed = [], 0.0, None, 0.0, None
+        chem = fall = iters = relaxed = 0
+        for k in range(steps):
+            e0.record(stream)
+            try:
+                s.step(stream=stream.cuda_stream)
+            except Exception as e:            # noqa: BLE001 - a flagged state ends the run
+                failed = f"step {k}: {e}"
+                break
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            pr = s.probe(stream=stream.cuda_stream)
+            st = s.relax_stats()
+            chem += st["nChem"]
+            fall += st["nFallback"]
+            iters += st["nIter"]
+            relaxed += st["nChem"] + st["nTherm"]
+            t = s.time()[1]
+            if tc is None:
+                pk = max(pk, pr["maxPressure"])
+                if hist and pr["vapourVolume"] < 0.1 * v0:
+                    tp, vp = hist[-1][0], hist[-1][1]
+                    tc = tp + (t - tp) * (vp - 0.1 * v0) / (vp - pr["vapourVolume"])
+            hist.append((t, pr["vapourVolume"], pr["maxPressure"]))
+        try:
+            s.check_state()
+        except Exception as e:                # noqa: BLE001
+            failed = failed or str(e)
         U = s.get_state()
-        s.profile(True)
-        time_steps(s, 2, torch, stream)
-        prof = s.profile_read()
-        s.profile(False)
+        data = s.relax_log_read(log) if log else None
         s.close()
-        return ms, prof, st, U, data
+        done = len(hist)
+        return dict(ms=ms, steps=done, U=U, hist=hist, tc=tc, peak=pk, failed=failed, chem=chem, fall=fall,
+                    iters_per_cell=iters / max(1, relaxed), data=data, v0=v0)
 
-    ms64, p64, st64, U64, (X, Y) = run("fp64", log=4_000_000)
-    res["fp64_value"] = nE * 3 * steps / (ms64 / 1e3)
-    res["fp64_relax_ms"] = p64["relax"]["ms"] / p64["relax"]["launches"]
+    def summary(r):
+        out = {"value": nE * case.rkSteps * r["steps"] / (r["ms"] / 1e3), "steps_run": r["steps"],
+               "collapse_time_s": r["tc"], "peak_pressure_pa": r["peak"],
+               "chem_cells_per_step": r["chem"] / max(1, r["steps"]),
+               "newton_iters_per_relaxed_cell": r["iters_per_cell"]}
+        if r["failed"]:
+            out["stopped"] = r["failed"][:200]
+        return out
+
+    r64 = run("fp64", log=12_000_000)
+    X, Y = r64.pop("data")
+    res["fp64"] = summary(r64)
     g = Surrogate(device=dev, seed=1)
     t0 = time.perf_counter()
-    take = min(len(X), 1_000_000)
+    take = min(len(X), 10_000_000)
     g.set_data(X[:take], Y[:take])
-    loss = g.train(15, batch=2048, lr=2e-3, seed=2)
-    res["surrogate_training"] = {"samples": take, "epochs": 15, "final_loss": loss,
+    epochs = 8
+    loss = g.train(epochs, batch=4096, lr=2e-3, seed=2)
+    res["surrogate_training"] = {"samples": take, "logged": int(len(X)), "epochs": epochs, "final_loss": loss,
                                  "seconds": time.perf_counter() - t0}
-    msm, pm, stm, Um, _ = run("mixed")
-    mss, ps, sts, Us, _ = run("mixed", sg=g)
-    res["mixed_value"] = nE * 3 * steps / (msm / 1e3)
-    res["mixed_relax_ms"] = pm["relax"]["ms"] / pm["relax"]["launches"]
-    res["value"] = nE * 3 * steps / (mss / 1e3)
-    res["relax_ms"] = ps["relax"]["ms"] / ps["relax"]["launches"]
-    res["mixed_surrogate_over_fp64"] = res["value"] / res["fp64_value"]
-    res["chem_cells"] = sts["nChem"]
-    res["fallback_rate"] = sts["nFallback"] / max(1, sts["nChem"])
-    res["newton_iters_per_cell"] = {"fp64_newton": st64["nIter"] / max(1, st64["nChem"] + st64["nTherm"]),
-                                    "mixed_newton": stm["nIter"] / max(1, stm["nChem"] + stm["nTherm"]),
-                                    "mixed_surrogate": sts["nIter"] / max(1, sts["nChem"] + sts["nTherm"])}
-    rho = lambda U: U[:, 1] + U[:, 2]
-    res["rho_rel_l2_vs_fp64"] = float(np.linalg.norm(rho(Us) - rho(U64)) / np.linalg.norm(rho(U64)))
-
-    def p_liq(U):
-        al = np.clip(U[:, 0], case.avfMin / 100, 1 - case.avfMin / 100)
-        r = U[:, 1] / al
-        gm = case.gamma[0]
-        return (gm - 1) * r * (U[:, 6] / U[:, 1]) - gm * case.pInf[0] - (gm - 1) * case.eta[0] * r
-
-    res["p_rel_l2_vs_fp64"] = float(np.linalg.norm(p_liq(Us) - p_liq(U64)) / np.linalg.norm(p_liq(U64)))
+    del X, Y
+    rm = run("mixed")
+    res["mixed"] = summary(rm)
+    rs = run("mixed", sg=g)
+    res["mixed_surrogate"] = summary(rs)
     g.close()
+    res["value"] = res["mixed_surrogate"]["value"]
+    res["fp64_value"] = res["fp64"]["value"]
+    res["mixed_surrogate_over_fp64"] = res["value"] / res["fp64_value"]
+    res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64_value"]
+    res["fallback_rate"] = rs["fall"] / max(1, rs["chem"])
+    res["history_fp64"] = {"every": 50, "t_s": [h[0] for h in r64["hist"][::50]],
+                           "vapour_volume": [h[1] for h in r64["hist"][::50]],
+                           "max_pressure": [h[2] for h in r64["hist"][::50]], "initial_vapour_volume": r64["v0"]}
+    # accuracy of the fast paths against the FP64 Newton run: the same number of steps
+    acc = {}
+    for key, r in (("mixed", rm), ("mixed_surrogate", rs)):
+        e = {}
+        if r["steps"] == r64["steps"]:
+            fe = field_errors(case, r["U"], r64["U"])
+            e = {k: fe[k] for k in ("rho", "p") if k in fe}
+        if r["tc"] is not None and r64["tc"] is not None:
+            e["collapse_time_rel_err"] = abs(r["tc"] - r64["tc"]) / r64["tc"]
+        if r64["peak"] > 0:
+            e["peak_pressure_rel_err"] = abs(r["peak"] - r64["peak"]) / r64["peak"]
+        acc[key] = e
+    acc["tolerance"] = {"rel_l2": 1e-4, "note": "rho / p relative L2 after the run against the FP64 Newton run"}
+    res["accuracy_vs_fp64"] = acc
     mesh.close()
     return res
 
 
-def cpu_baseline(mesh, case, U, max_stages=3):
-    """FP64 CPU restatement (oracle) on all host threads: full RK stages on the same mesh."""
+def cpu_baseline(view, case, U, steps=2):
+    """FP64 CPU restatement (oracle) on all host threads: `steps` full explicitLoop steps (dt,
+    3 RK stages, relaxation, conservation) on the full mesh.  Returns the baseline record and the
+    final state (the accuracy check compares the GPU paths with it)."""
     from oracle import oracle_py as O
     th = os.cpu_count() or 1
     O.set_threads(th)
-    o = O.Oracle(mesh.view(), case)
+    o = O.Oracle(view, case)
     Uc = U.copy()
-    o.residual(Uc)  # warm-up (builds the per-cell face lists)
     t0 = time.perf_counter()
-    stages = 0
-    o.init_rk(Uc)
-    while stages < max_stages:
-        o.residual(Uc)
-        o.update(stages % 3, 1e-4, Uc)
-        stages += 1
-        if time.perf_counter() - t0 > 60:
-            break
+    for _ in range(steps):
+        o.step(Uc)
     dt = time.perf_counter() - t0
     o.close()
-    return {"value": mesh.n_elem * stages / dt, "unit": UNIT, "cores": th, "kind": "port",
-            "sample": f"{stages} RK3 stages (residual + update, FP64) on the full {mesh.n_elem}-cell mesh"}
+    rec = {"value": view.nElem * case.rkSteps * steps / dt, "unit": UNIT, "cores": th, "kind": "port",
+           "sample": f"{steps} explicitLoop steps ({case.rkSteps} RK stages + relaxation each, FP64) on the full "
+                     f"{view.nElem}-cell mesh, {dt:.1f} s"}
+    return rec, Uc
+
+
+FIELDS = ["alpha", "alpha_rhoL", "alphaG_rhoG", "rho_u", "rho_v", "rho_w", "alpha_rhoL_eL", "alphaG_rhoG_eG",
+          "rho_E", "vapour_mass"]
+
+
+def field_errors(case, U, Uref) -> dict:
+    """Relative L2 and Linf error per field of U against Uref (reference order): the ten conserved
+    variables (momentum components normalised by the whole momentum field), the mixture density
+    and the mixture pressure.  Fields that are zero everywhere in Uref are left out."""
+    from fooskagpu_b200 import cases
+    out = {}
+    mom_l2, mom_inf = np.linalg.norm(Uref[:, 3:6]), np.abs(Uref[:, 3:6]).max()
+    cols = [(FIELDS[v], U[:, v], Uref[:, v], v) for v in range(10)]
+    cols.append(("rho", U[:, 1] + U[:, 2], Uref[:, 1] + Uref[:, 2], -1))
+    cols.append(("p", cases.mixture_pressure(case, U), cases.mixture_pressure(case, Uref), -1))
+    for name, a, b, v in cols:
+        l2n, infn = (mom_l2, mom_inf) if 3 <= v <= 5 else (np.linalg.norm(b), np.abs(b).max())
+        if infn == 0:
+            continue
+        d = a - b
+        out[name] = {"rel_l2": float(np.linalg.norm(d) / l2n), "rel_linf": float(np.abs(d).max() / infn)}
+    return out
+
+
+# tolerances of the accuracy checks (relative L2 / Linf per field against the FP64 oracle): the
+# FP64 path differs from the oracle by summation order and FMA contraction; the mixed path by its
+# FP32 face math (~1e-7 relative per stage)
+ACC_TOL = {"fp64": {"rel_l2": 1e-9, "rel_linf": 1e-6}, "mixed": {"rel_l2": 1e-5, "rel_linf": 1e-4}}
+
+
+def accuracy(mesh, case, U0, Uref, steps, dev, torch, stream) -> dict:
+    """Both GPU paths run the oracle's `steps` explicitLoop steps from the same state; per-field
+    errors against the oracle's state and the stated tolerance."""
+    from fooskagpu_b200.api import Solver
+    res = {"steps": steps, "against": "FP64 oracle (CPU restatement of the reference solver), same mesh, same state",
+           "tolerance": ACC_TOL}
+    for prec in ("fp64", "mixed"):
+        s = Solver(mesh, case, precision=prec, device=dev)
+        s.set_state(U0)
+        for _ in range(steps):
+            s.step(stream=stream.cuda_stream)
+        U = s.get_state(stream=stream.cuda_stream)
+        s.close()
+        e = field_errors(case, U, Uref)
+        tol = ACC_TOL[prec]
+        res[prec] = {"fields": e, "pass": all(x["rel_l2"] <= tol["rel_l2"] and x["rel_linf"] <= tol["rel_linf"]
+                                              for x in e.values())}
+    return res
 
 
 def reference_gpu(args):
@@ -412,32 +542,27 @@ def reference_gpu(args):
     same 128^3 hex cube, TGV state and case, with slip walls in place of the periodic faces
     (the reference has no periodic boundary), elements in the same shuffled order (the reference
     does not renumber).  Timed by CUDA events that oracle/ref_driver.cu records around its step
-    loop."""
+    loop (the end event after a device-wide synchronisation).  Nothing of this repository's
+    product runs here: the mesh centres for the initial state come from the oracle's mesh
+    restatement."""
     from oracle import ref_run
     if not ref_run.available():
         return {"unavailable": "reference GPU build oracle/_ref/fooska_ref_dp not present (built from the reference sources)"}
-    try:
-        import torch
-        if not torch.cuda.is_available():
-            return {"unavailable": "no GPU visible"}
-    except Exception as e:  # pragma: no cover
-        return {"unavailable": f"torch: {e}"}
     from fooskagpu_b200 import cases, meshgen
-    from fooskagpu_b200.api import Mesh
+    from oracle import oracle_mesh
+    from oracle.ref_case import reference_defaults
     L = 2 * math.pi
     MESH_DIR.mkdir(parents=True, exist_ok=True)
     path = MESH_DIR / f"tgv{NCELL_SIDE}_slip_shuffled.neu"
+    nm = meshgen.box_hexes(NCELL_SIDE, NCELL_SIDE, NCELL_SIDE, L=(L, L, L), shuffle=True, seed=20261203)
     if not path.exists():
-        meshgen.write_neu(str(path), meshgen.box_hexes(NCELL_SIDE, NCELL_SIDE, NCELL_SIDE, L=(L, L, L), shuffle=True,
-                                                       seed=20261203))
-    mesh = Mesh.load_neu(str(path), scale=1.0)
-    case = cases.tgv_case()
-    U = cases.tgv_ic(case, mesh.arrays()["cellCenter"])
-    nE = mesh.n_elem
-    mesh.close()
-    steps, warm = max(1, min(args.steps, 20)), 3
+        meshgen.write_neu(str(path), nm)
+    case = bench_tgv_case(base=reference_defaults())
+    U = cases.tgv_ic(case, oracle_mesh.build(nm.nodes, nm.elems, nm.bcs).cellCenter)
+    nE = len(U)
+    steps, warm = max(1, args.steps), args.warmup
     try:
-        rep = ref_run.run(MESH_DIR / "ref_workdir", path, case, U, steps, warm, timeout=600)
+        rep = ref_run.run(MESH_DIR / "ref_workdir", path, case, U, steps, warm, timeout=900)
     except Exception as e:
         return {"unavailable": f"reference GPU run failed: {str(e)[:300]}"}
     ms = rep["ms"]
@@ -449,45 +574,42 @@ def reference_gpu(args):
 
 
 def run_reference(args):
-    """Reference arm: the reference's path has no CPU implementation of its own, so this times
-    the FP64 CPU restatement of it (oracle) with all host threads on the same workload."""
-    from fooskagpu_b200 import cases
-    from fooskagpu_b200.api import Mesh
-    path, per = tgv_mesh(0, 1, None)
-    mesh = Mesh.load_neu(path, scale=1.0, periodic=per)
-    case = cases.tgv_case()
-    U = cases.tgv_ic(case, mesh.arrays()["cellCenter"])
-    from oracle import oracle_py as O
+    """Reference arm.  The reference implements this path only in CUDA, so its CPU arm is the FP64
+    C++ restatement of it (oracle), on all host threads, on the same workload: the same mesh
+    (built by the oracle's own numpy restatement of the reference's pre-processing), the same
+    case and initial state, the same warm-up and timed step counts (full explicitLoop steps).
+    Nothing of this repository's product library is loaded.  The line also carries the
+    reference's own CUDA build run on the same GPU (reference_gpu)."""
+    from fooskagpu_b200 import cases, meshgen
+    from oracle import oracle_mesh, oracle_py as O
+    from oracle.ref_case import reference_defaults
+    L = 2 * math.pi
+    nm = meshgen.box_hexes(NCELL_SIDE, NCELL_SIDE, NCELL_SIDE, L=(L, L, L), side_bc={}, shuffle=True, seed=20261203)
+    om = oracle_mesh.build(nm.nodes, nm.elems, nm.bcs, periodic=(L, L, L))
+    del nm
+    case = bench_tgv_case(base=reference_defaults())
+    U = cases.tgv_ic(case, om.cellCenter)
     th = os.cpu_count() or 1
     O.set_threads(th)
-    o = O.Oracle(mesh.view(), case)
+    o = O.Oracle(om.view(), case)
     Uc = U.copy()
-    tw = time.perf_counter()
-    o.init_rk(Uc)
-    for w in range(args.warmup):   # warm-up stages on a copy of the state
-        o.residual(Uc)
-        o.update(w % 3, 1e-4, Uc)
-        if time.perf_counter() - tw > 60:
-            break
-    Uc = U.copy()
-    steps = 0
-    cap = max(1, min(args.steps, args.cpu_stages))
+    for _ in range(args.warmup):
+        o.step(Uc)
     t0 = time.perf_counter()
-    o.init_rk(Uc)
-    while steps < cap:
-        o.residual(Uc)
-        o.update(steps % 3, 1e-4, Uc)
-        steps += 1
-        if time.perf_counter() - t0 > 90:
-            break
+    for _ in range(args.steps):
+        o.step(Uc)
     dt = time.perf_counter() - t0
-    val = mesh.n_elem * steps / dt
-    sample = f"{steps} RK3 stages (one stage per step) on the full {mesh.n_elem}-cell mesh"
+    o.close()
+    val = om.nElem * case.rkSteps * args.steps / dt
+    sample = (f"{args.steps} explicitLoop steps ({case.rkSteps} RK stages + relaxation each) after {args.warmup} "
+              f"warm-up steps on the full {om.nElem}-cell mesh")
     return dict(
-        impl="reference", metric=METRIC, value=val, unit=UNIT, n_gpus=1, steps=steps, warmup=args.warmup,
-        ms_per_step=dt * 1e3 / steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+        impl="reference", metric=METRIC, value=val, unit=UNIT, n_gpus=1, steps=args.steps, warmup=args.warmup,
+        ms_per_step=dt * 1e3 / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
         data="synthetic",
-        config={"workload": f"tgv_les_wale_{NCELL_SIDE}^3_hex_periodic", "cells": mesh.n_elem, "rk_stages": 3},
+        config={"workload": f"tgv_les_wale_{NCELL_SIDE}^3_hex_periodic", "cells": om.nElem, "faces": om.nFcs,
+                "rk_stages": case.rkSteps,
+                "dt": f"adaptive every {TGV_DT_EVERY} steps (CFL 0.5)"},
         cpu_baseline={"kind": "port", "cores": th, "sample": sample, "value": val, "unit": UNIT},
         e2e={"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         note="the reference implements this path only in CUDA; its CPU arm is the FP64 C++ restatement (oracle)",
@@ -501,7 +623,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-stages", type=int, default=6)
+    ap.add_argument("--cpu-steps", type=int, default=2, help="oracle steps of the CPU baseline / accuracy check")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="reference arm: skip timing the reference GPU build")
     ap.add_argument("--no-two-phase", action="store_true", help="skip the two-phase (surrogate) workload")

@@ -42,13 +42,18 @@ class FgCase(C.Structure):
         ("pInf", f64 * 2), ("gamma", f64 * 2), ("Cp", f64 * 2), ("eta", f64 * 2), ("satConst", f64 * 2),
         ("dynVisc", f64 * 2), ("heatCoef", f64 * 2), ("Pr", f64 * 2),
         ("relaxFlag", i32), ("hllcEnergyFix", i32), ("hllcTieTol", f64), ("heatFlux", i32),
-        ("limiter", i32), ("inletVelFlag", i32), ("reserved", i32 * 3), ("inletVel", f64 * 3),
+        ("limiter", i32), ("inletVelFlag", i32), ("inletStateFlag", i32), ("reserved", i32 * 2),
+        ("inletVel", f64 * 3), ("inletP", f64), ("inletT", f64),
     ]
 
 
 class FgMeshOpts(C.Structure):
     _fields_ = [("scale", f64), ("periodic", f64 * 3), ("renumber", i32), ("gpu", i32), ("device", i32),
                 ("reserved", i32 * 1)]
+
+
+class FgProbe(C.Structure):
+    _fields_ = [("vapourVolume", f64), ("maxPressure", f64), ("minPressure", f64), ("maxSpeed", f64)]
 
 
 class FgMeshInfo(C.Structure):
@@ -93,6 +98,7 @@ SIGNATURES = {
     "fg_last_error": (C.c_char_p, []),
     "fg_case_default": (None, [C.POINTER(FgCase)]),
     "fg_mesh_load_neu": (C.c_int, [C.c_char_p, C.POINTER(FgMeshOpts), C.POINTER(VP)]),
+    "fg_mesh_build": (C.c_int, [i32, PD, i32, PI, PI, PI, C.POINTER(FgMeshOpts), C.POINTER(VP)]),
     "fg_mesh_info_get": (C.c_int, [VP, C.POINTER(FgMeshInfo)]),
     "fg_mesh_view_get": (C.c_int, [VP, C.POINTER(FgMeshView)]),
     "fg_mesh_permutation": (C.c_int, [VP, PI, i32]),
@@ -105,7 +111,9 @@ SIGNATURES = {
     "fg_solver_create": (C.c_int, [VP, C.POINTER(FgCase), i32, i32, C.POINTER(VP)]),
     "fg_solver_destroy": (C.c_int, [VP]),
     "fg_solver_memory": (C.c_int, [VP, C.POINTER(C.c_uint64)]),
+    "fg_probe": (C.c_int, [VP, C.POINTER(FgProbe), VP]),
     "fg_set_state": (C.c_int, [VP, PD, VP]),
+    "fg_set_state_async": (C.c_int, [VP, PD, VP]),
     "fg_get_state": (C.c_int, [VP, PD, VP]),
     "fg_compute_rhs": (C.c_int, [VP, i32, VP]),
     "fg_compute_time_step": (C.c_int, [VP, PD, VP]),

@@ -62,6 +62,38 @@ class Mesh:
         check(lib().fg_mesh_load_neu(path.encode(), C.byref(o), C.byref(h)))
         return cls(h)
 
+    @classmethod
+    def build(cls, nodes: np.ndarray, elems, bcs: dict, scale: float = 1.0, periodic=(0.0, 0.0, 0.0),
+              renumber: str = "morton", gpu: bool = False, device: int = 0) -> "Mesh":
+        """The same pre-processing for element lists held in memory (fg_mesh_build): nodes
+        (nNodes, 3); elems, a list of (nE_k, nn_k) 0-based node-id blocks in element order; bcs,
+        {name: (gambit code, element ids, local faces)} as meshgen.NeuMesh holds them."""
+        code_map = {45: 1, 26: 2, 13: 3, 42: 4, 51: 5}
+        n_elem = sum(len(b) for b in elems)
+        el_nn = np.empty(n_elem, dtype=np.int32)
+        el_nodes = np.zeros((n_elem, 8), dtype=np.int32)
+        off = 0
+        for b in elems:
+            el_nn[off:off + len(b)] = b.shape[1]
+            el_nodes[off:off + len(b), :b.shape[1]] = b
+            off += len(b)
+        el_bc = np.zeros((n_elem, 6), dtype=np.int32)
+        for _, (code, el, fc) in bcs.items():
+            if code in code_map:
+                el_bc[np.asarray(el), np.asarray(fc)] = code_map[code]
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        o = FgMeshOpts()
+        o.scale = scale
+        for d in range(3):
+            o.periodic[d] = periodic[d]
+        o.renumber = _RENUM[renumber]
+        o.gpu = 1 if gpu else 0
+        o.device = device
+        h = C.c_void_p()
+        check(lib().fg_mesh_build(len(nodes), _dptr(nodes), n_elem, el_nn.ctypes.data_as(L.PI),
+                                  el_nodes.ctypes.data_as(L.PI), el_bc.ctypes.data_as(L.PI), C.byref(o), C.byref(h)))
+        return cls(h)
+
     def view(self) -> FgMeshView:
         v = FgMeshView()
         check(lib().fg_mesh_view_get(self._h, C.byref(v)))
@@ -140,6 +172,13 @@ class Solver:
     def set_state(self, U: np.ndarray, stream: Optional[int] = None) -> None:
         U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.n, 10)
         check(lib().fg_set_state(self._h, _dptr(U), stream))
+
+    def set_state_async(self, U: np.ndarray, stream: Optional[int] = None) -> None:
+        """Queue the upload without synchronising (fg_set_state_async); U must stay unchanged
+        until the stream has passed the copy when it is pinned memory."""
+        if not (U.dtype == np.float64 and U.flags["C_CONTIGUOUS"] and U.shape == (self.n, 10)):
+            raise ValueError("set_state_async needs a C-contiguous float64 array of shape (n, 10)")
+        check(lib().fg_set_state_async(self._h, _dptr(U), stream))
 
     def get_state(self, out: Optional[np.ndarray] = None, stream: Optional[int] = None) -> np.ndarray:
         if out is None:
@@ -242,6 +281,12 @@ class Solver:
         k = C.c_int64()
         check(lib().fg_relax_log_read(self._h, _fptr(X), _fptr(Y), int(cap), C.byref(k)))
         return X[:k.value].copy(), Y[:k.value].copy()
+
+    def probe(self, stream=None) -> dict:
+        """Vapour volume, max / min mixture pressure and max speed of the current state."""
+        pr = L.FgProbe()
+        check(lib().fg_probe(self._h, C.byref(pr), stream))
+        return {k: getattr(pr, k) for k, _ in L.FgProbe._fields_}
 
     def cons_calc(self, ivar: int, stream=None) -> float:
         v = C.c_double()

@@ -23,6 +23,55 @@ constexpr int GREC = 36;
 constexpr int NV = 10;
 constexpr int MAXSLOT = 6;
 
+// ---------------------------------------------------------------- record layout
+// The per-cell records (W: WREC values, G: GREC values) are stored component-major in 16-byte
+// vectors: vector q of cell c (values q * VPV .. q * VPV + VPV - 1, VPV = 16 / sizeof(T)) sits at
+// base + (q * stride + c) * VPV, stride = the number of cells with records.  A warp that reads
+// one vector of consecutive or nearby cells (the owners of consecutive faces, the Morton-ordered
+// neighbours) touches a few cache lines instead of one line per lane as with whole records.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; };
+template <> struct Vec16<double> { using type = double2; };
+template <typename T>
+__host__ __device__ constexpr int vpv() { return 16 / (int)sizeof(T); }
+// index of value v of cell c
+template <typename T>
+__host__ __device__ inline size_t rec_index(size_t stride, size_t c, int v) {
+    return ((size_t)(v / vpv<T>()) * stride + c) * vpv<T>() + (size_t)(v % vpv<T>());
+}
+// lane j of a 16-byte vector (no address of a vector is taken, so the vectors stay in registers)
+__device__ __forceinline__ float vlane(const float4 &x, int j) { return j == 0 ? x.x : j == 1 ? x.y : j == 2 ? x.z : x.w; }
+__device__ __forceinline__ double vlane(const double2 &x, int j) { return j == 0 ? x.x : x.y; }
+// the first NVAL values of the record of cell c
+template <typename T, int NVAL>
+__device__ __forceinline__ void rec_load(const T *__restrict__ base, size_t stride, int c, T *out) {
+    using V = typename Vec16<T>::type;
+    constexpr int P = vpv<T>();
+    const V *b = reinterpret_cast<const V *>(base);
+#pragma unroll
+    for (int q = 0; q < (NVAL + P - 1) / P; q++) {
+        const V x = __ldg(b + (size_t)q * stride + c);
+#pragma unroll
+        for (int j = 0; j < P; j++)
+            if (q * P + j < NVAL) out[q * P + j] = vlane(x, j);
+    }
+}
+// store NVAL values as the record of cell c (the rest of the last vector is zero)
+template <typename T, int NVAL>
+__device__ __forceinline__ void rec_store(T *base, size_t stride, int c, const T *in) {
+    using V = typename Vec16<T>::type;
+    constexpr int P = vpv<T>();
+    V *b = reinterpret_cast<V *>(base);
+    auto val = [&](int i) { return i < NVAL ? in[i] : (T)0; };
+#pragma unroll
+    for (int q = 0; q < (NVAL + P - 1) / P; q++) {
+        V x;
+        if constexpr (P == 4) x = make_float4(val(4 * q), val(4 * q + 1), val(4 * q + 2), val(4 * q + 3));
+        else x = make_double2(val(2 * q), val(2 * q + 1));
+        b[(size_t)q * stride + c] = x;
+    }
+}
+
 template <typename T>
 struct PhysT {
     T gam[2], gm1[2], gp1[2], pinf[2], gpinf[2], cvgm1[2], gm1eta[2], mu[2];

@@ -21,63 +21,6 @@ namespace fg {
 
 
 template <typename T>
-__device__ __forceinline__ void load_rec(const T *__restrict__ W, int c, T *w) {
-    const T *p = W + (size_t)c * WREC;
-#pragma unroll
-    for (int v = 0; v < NP; v++) w[v] = __ldg(p + v);
-}
-template <>
-__device__ __forceinline__ void load_rec<float>(const float *__restrict__ W, int c, float *w) {
-    const float4 *p = reinterpret_cast<const float4 *>(W + (size_t)c * WREC);
-    const float4 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2);
-    w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
-    w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
-    w[8] = d.x;
-}
-template <typename T>
-__device__ __forceinline__ void store_rec(T *W, int c, const T *w) {
-    T *p = W + (size_t)c * WREC;
-#pragma unroll
-    for (int v = 0; v < NP; v++) p[v] = w[v];
-#pragma unroll
-    for (int v = NP; v < WREC; v++) p[v] = 0;
-}
-template <>
-__device__ __forceinline__ void store_rec<float>(float *W, int c, const float *w) {
-    float4 *p = reinterpret_cast<float4 *>(W + (size_t)c * WREC);
-    p[0] = make_float4(w[0], w[1], w[2], w[3]);
-    p[1] = make_float4(w[4], w[5], w[6], w[7]);
-    p[2] = make_float4(w[8], 0.f, 0.f, 0.f);
-}
-template <typename T>
-__device__ __forceinline__ void load_g(const T *__restrict__ G, int c, T *g) {
-    const T *p = G + (size_t)c * GREC;
-#pragma unroll
-    for (int v = 0; v < GREC; v++) g[v] = __ldg(p + v);
-}
-template <>
-__device__ __forceinline__ void load_g<float>(const float *__restrict__ G, int c, float *g) {
-    const float4 *p = reinterpret_cast<const float4 *>(G + (size_t)c * GREC);
-#pragma unroll
-    for (int q = 0; q < GREC / 4; q++) {
-        const float4 t = __ldg(p + q);
-        g[4 * q + 0] = t.x; g[4 * q + 1] = t.y; g[4 * q + 2] = t.z; g[4 * q + 3] = t.w;
-    }
-}
-template <typename T>
-__device__ __forceinline__ void store_g(T *G, int c, const T *g) {
-    T *p = G + (size_t)c * GREC;
-#pragma unroll
-    for (int v = 0; v < GREC; v++) p[v] = g[v];
-}
-template <>
-__device__ __forceinline__ void store_g<float>(float *G, int c, const float *g) {
-    float4 *p = reinterpret_cast<float4 *>(G + (size_t)c * GREC);
-#pragma unroll
-    for (int q = 0; q < GREC / 4; q++) p[q] = make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]);
-}
-
-template <typename T>
 __device__ __forceinline__ void store_frec(T *FB, int f, const T *r) {
     T *p = FB + (size_t)f * FREC;
 #pragma unroll
@@ -114,10 +57,6 @@ __device__ __forceinline__ void load_frec<float>(const float *__restrict__ FB, i
 // of words so that threads of a warp reading the same field of consecutive cells hit distinct
 // banks.  slotLocal holds the neighbour's staged-record index, or -bc on a boundary slot.
 constexpr int kGeoComp = 6;    // aox aoy aoz dcx dcy dcz
-
-template <typename T> struct Vec16;
-template <> struct Vec16<float> { using type = float4; };
-template <> struct Vec16<double> { using type = double2; };
 
 // record area rounded up to 16 bytes so the staged geometry arrays start aligned
 template <typename T>
@@ -213,20 +152,20 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     T *sg = reinterpret_cast<T *>(smem_raw + rec_area<T>(m, WS));   // kGeoComp * B * nSlots
     int *sl = reinterpret_cast<int *>(sg + (size_t)kGeoComp * B * m.nSlots);
     {
-        // each lane copies one 16-byte vector of a W record (WREC / TPV vectors per record)
+        // each lane copies one 16-byte vector of a W record; consecutive lanes take the same
+        // vector of consecutive staged cells (contiguous for the block's own cells)
         using V = typename Vec16<T>::type;
-        constexpr int TPV = 16 / sizeof(T);
-        constexpr int WV = WREC / TPV;
+        constexpr int TPV = vpv<T>();
+        constexpr int WV = (NP + TPV - 1) / TPV;   // vectors holding the NP used values
         const V *Wv = reinterpret_cast<const V *>(W);
         for (int i = threadIdx.x; i < nRec * WV; i += blockDim.x) {
-            const int r = i / WV, q = i - (i / WV) * WV;
+            const int q = i / nRec, r = i - q * nRec;
             const int src = staged_source(m, b, r, lo, nBlockRecs);
             if (src < 0) continue;
-            const V x = __ldg(Wv + (size_t)src * WV + q);
-            const T *xs = reinterpret_cast<const T *>(&x);
+            const V x = __ldg(Wv + (size_t)q * m.n + src);
 #pragma unroll
             for (int j = 0; j < TPV; j++)
-                if (q * TPV + j < NP) rec[r * WS + q * TPV + j] = xs[j];
+                if (q * TPV + j < NP) rec[r * WS + q * TPV + j] = vlane(x, j);
         }
     }
     stage_geometry(m, lo, nOwn, sg, sl);
@@ -303,7 +242,7 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     for (int v = 0; v < NP; v++) out[v] = th[v];
 #pragma unroll
     for (int q = 0; q < NP * 3; q++) out[NP + q] = gs[q];
-    store_g(G, c, out);
+    rec_store<T, GREC>(G, m.n, c, out);
 }
 
 // MUSCL face state of a cell: w + theta * ((x_f - x_c) . grad w)  (DP/computeFaceValues.cu:66-105)
@@ -327,58 +266,14 @@ __device__ __forceinline__ void cell_grad_t(const PhysT<T> &P, const T *w, const
     for (int d = 0; d < 3; d++) acc[d] += (g[NP + 3 * 6 + d] - c * g[NP + 3 * 1 + d]) * inv;
 }
 
-// ------------------------------------------------------------------ face flux (once per face)
-// Record of face f with canonical normal n (owner -> neighbour), area A:
-//   H[v] = A (F[v] - Visc[v]) + A pF n (momentum),  u = A (u* . n),  signal
-// where F is the HLLC + advective flux (DP/computeRHS.cu:117-131), Visc the WALE viscous flux
-// (DP/computeViscousStresses.cu:87-170) and pF the upwind mixture pressure.  A cell with
-// orientation s (-1 owner, +1 neighbour, the reference's sign) receives s * H[v] plus its
-// cell-centre terms, which k_gather adds from sums over its faces:
-//   var 0: -alpha_c s u,  vars 6/7: +alpha_c pL_c s u, +(1-alpha_c) pG_c s u,
-//   momentum: -pC_c s A n summed = pC_c * (sum of outward n A)  (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
+// Flux part of a face, shared by the face kernels: HLLC + pressure + viscous (+ heat) flux of the
+// reconstructed states sL (owner) and sR (neighbour or ghost), written as the face record of fi.
+// p1: neighbour state for the viscous flux (the cell-centre ghost on a boundary face);
+// gO / gN: the two cells' velocity gradients; gT: sum of their temperature gradients.
 template <typename T>
-__global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
-                                              T *__restrict__ FB, const PhysT<T> P, int wantSignal) {
-    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (fi >= m.nF) return;
-    const int o = m.fOwn[fi];
-    const int nb = m.fNb[fi];
-    const T nx = m.fnx[fi], ny = m.fny[fi], nz = m.fnz[fi], A = m.fA[fi];
-    T wo[NP], sL[NP], sR[NP], p1[NP], gO[9], gN[9];
-    T gT[3] = {0, 0, 0};   // sum of the two cells' temperature gradients (heat conduction)
-    {
-        T g[GREC];
-        load_rec(W, o, wo);
-        load_g(G, o, g);
-        face_state(wo, g, m.fdo[0][fi], m.fdo[1][fi], m.fdo[2][fi], sL);
-#pragma unroll
-        for (int q = 0; q < 9; q++) gO[q] = g[NP + 9 + q];
-        if (P.heat && nb >= 0) cell_grad_t(P, wo, g, gT);
-    }
-    if (nb >= 0) {
-        T wn[NP], g[GREC];
-        load_rec(W, nb, wn);
-        load_g(G, nb, g);
-        face_state(wn, g, m.fdn[0][fi], m.fdn[1][fi], m.fdn[2][fi], sR);
-#pragma unroll
-        for (int q = 0; q < 9; q++) gN[q] = g[NP + 9 + q];
-        if (P.heat) cell_grad_t(P, wn, g, gT);
-#pragma unroll
-        for (int v = 0; v < NP; v++) p1[v] = sR[v];
-    } else {
-        // ghost of the reconstructed state for the flux (DP/computeRHS.cu:113); the viscous flux
-        // reads the ghost of the cell-centre state (DP/computePrimVec.cu:61-76) and the owner's
-        // gradient twice
-#pragma unroll
-        for (int v = 0; v < NP; v++) {
-            sR[v] = sL[v];
-            p1[v] = wo[v];
-        }
-        ghost_state(P, -nb, nx, ny, nz, sR);
-        ghost_state(P, -nb, nx, ny, nz, p1);
-#pragma unroll
-        for (int q = 0; q < 9; q++) gN[q] = gO[q];
-    }
+__device__ __forceinline__ void face_tail(const PhysT<T> &P, const T *sL, const T *sR, const T *p1, const T *gO,
+                                          const T *gN, const T *gT, int nb, T nx, T ny, T nz, T A, T lsSq,
+                                          int wantSignal, T *__restrict__ FB, int fi) {
     T F[NV], unc, pF;
     hllc_flux(P, sL, sR, nx, ny, nz, F, unc, pF);
     T H[NV];
@@ -391,7 +286,7 @@ __global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(co
         T gv[9];
 #pragma unroll
         for (int q = 0; q < 9; q++) gv[q] = (gO[q] + gN[q]) * (T)0.5;
-        const T nut = P.turb ? wale_nu(gv, m.fLsSq[fi]) : (T)0;
+        const T nut = P.turb ? wale_nu(gv, lsSq) : (T)0;
         const T dv = (gv[0] + gv[4] + gv[8]) * ((T)2 / 3);
         const T t00 = 2 * gv[0] - dv, t11 = 2 * gv[4] - dv, t22 = 2 * gv[8] - dv;
         const T t01 = gv[1] + gv[3], t02 = gv[2] + gv[6], t12 = gv[5] + gv[7];
@@ -427,6 +322,61 @@ __global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(co
     store_frec(FB, fi, rec);
 }
 
+// ------------------------------------------------------------------ face flux (once per face)
+// Record of face f with canonical normal n (owner -> neighbour), area A:
+//   H[v] = A (F[v] - Visc[v]) + A pF n (momentum),  u = A (u* . n),  signal
+// where F is the HLLC + advective flux (DP/computeRHS.cu:117-131), Visc the WALE viscous flux
+// (DP/computeViscousStresses.cu:87-170) and pF the upwind mixture pressure.  A cell with
+// orientation s (-1 owner, +1 neighbour, the reference's sign) receives s * H[v] plus its
+// cell-centre terms, which k_gather adds from sums over its faces:
+//   var 0: -alpha_c s u,  vars 6/7: +alpha_c pL_c s u, +(1-alpha_c) pG_c s u,
+//   momentum: -pC_c s A n summed = pC_c * (sum of outward n A)  (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
+template <typename T>
+__global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
+                                              T *__restrict__ FB, const PhysT<T> P, int wantSignal) {
+    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fi >= m.nF) return;
+    const int o = m.fOwn[fi];
+    const int nb = m.fNb[fi];
+    const T nx = m.fnx[fi], ny = m.fny[fi], nz = m.fnz[fi], A = m.fA[fi];
+    T wo[NP], sL[NP], sR[NP], p1[NP], gO[9], gN[9];
+    T gT[3] = {0, 0, 0};   // sum of the two cells' temperature gradients (heat conduction)
+    {
+        T g[GREC];
+        rec_load<T, NP>(W, m.n, o, wo);
+        rec_load<T, GREC>(G, m.n, o, g);
+        face_state(wo, g, m.fdo[0][fi], m.fdo[1][fi], m.fdo[2][fi], sL);
+#pragma unroll
+        for (int q = 0; q < 9; q++) gO[q] = g[NP + 9 + q];
+        if (P.heat && nb >= 0) cell_grad_t(P, wo, g, gT);
+    }
+    if (nb >= 0) {
+        T wn[NP], g[GREC];
+        rec_load<T, NP>(W, m.n, nb, wn);
+        rec_load<T, GREC>(G, m.n, nb, g);
+        face_state(wn, g, m.fdn[0][fi], m.fdn[1][fi], m.fdn[2][fi], sR);
+#pragma unroll
+        for (int q = 0; q < 9; q++) gN[q] = g[NP + 9 + q];
+        if (P.heat) cell_grad_t(P, wn, g, gT);
+#pragma unroll
+        for (int v = 0; v < NP; v++) p1[v] = sR[v];
+    } else {
+        // ghost of the reconstructed state for the flux (DP/computeRHS.cu:113); the viscous flux
+        // reads the ghost of the cell-centre state (DP/computePrimVec.cu:61-76) and the owner's
+        // gradient twice
+#pragma unroll
+        for (int v = 0; v < NP; v++) {
+            sR[v] = sL[v];
+            p1[v] = wo[v];
+        }
+        ghost_state(P, -nb, nx, ny, nz, sR);
+        ghost_state(P, -nb, nx, ny, nz, p1);
+#pragma unroll
+        for (int q = 0; q < 9; q++) gN[q] = gO[q];
+    }
+    face_tail(P, sL, sR, p1, gO, gN, gT, nb, nx, ny, nz, A, m.fLsSq[fi], wantSignal, FB, fi);
+}
+
 // ------------------------------------------------------------------ owner-side gather + RK
 template <typename T>
 __global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gather(const DevMesh<T> m, Fields<T> f, const PhysD D, int mode,
@@ -453,7 +403,7 @@ __global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gat
             sig = fmax(sig, rec[NV + 1]);
         }
         T w[NP];
-        load_rec(f.Win, c, w);
+        rec_load<T, NP>(f.Win, m.n, c, w);
         const double a = w[0], pl = w[6], pg = w[7];
         const double pc = (double)(w[0] * w[6] + (1 - w[0]) * w[7]);
         acc[0] -= a * su;
@@ -498,7 +448,7 @@ __global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gat
             if (!state_ok(u)) *f.bad = f.step + 1;
             T wo[NP];
             cons2prim_d(D, u, wo);
-            store_rec(f.Wout, c, wo);
+            rec_store<T, NP>(f.Wout, m.n, c, wo);
         }
     }
     if (wantSignal) {
@@ -543,11 +493,11 @@ __global__ void k_update(const DevMesh<T> m, Fields<T> f, const PhysD D, StageCo
     if (!state_ok(u)) *f.bad = f.step + 1;
     T wo[NP];
     cons2prim_d(D, u, wo);
-    store_rec(f.Wout, c, wo);
+    rec_store<T, NP>(f.Wout, m.n, c, wo);
 }
 
 template <typename T>
-__global__ void k_prim(int n, const double *__restrict__ U, T *W, const PhysD D) {
+__global__ void k_prim(int n, const double *__restrict__ U, T *W, size_t wStride, const PhysD D) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     double u[NV];
@@ -555,7 +505,7 @@ __global__ void k_prim(int n, const double *__restrict__ U, T *W, const PhysD D)
     for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
     T w[NP];
     cons2prim_d(D, u, w);
-    store_rec(W, c, w);
+    rec_store<T, NP>(W, wStride, c, w);
 }
 
 __global__ void k_dt_finalize(const double *blockMin, int nb, double cfl, double maxDt, double *dt) {
@@ -606,6 +556,70 @@ __global__ void k_cons_final(const double *blockSum, int nb, double *out) {
     if (threadIdx.x == 0) *out = sh[0];
 }
 
+// ------------------------------------------------------------------ state probe
+// Per block of kConsThreads cells: [0] sum of (1 - alpha) V (the vapour volume, the reference's
+// consCalc of variable 0), [1] max and [2] min of the mixture pressure alpha p_L + (1 - alpha) p_G,
+// [3] max speed |u|; then one block combines the block results in block order.  Deterministic.
+__global__ void k_probe_blocks(int n, const double *__restrict__ U, const double *__restrict__ vol, const PhysD D,
+                               double *blockOut) {
+    __shared__ double sh[4][kConsThreads];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double vv = 0.0, pmax = -1e300, pmin = 1e300, umax = 0.0;
+    if (c < n) {
+        double u[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
+        double w[NP];
+        cons2prim_d(D, u, w);
+        const double p = w[0] * w[6] + (1 - w[0]) * w[7];
+        vv = (1.0 - u[0]) * vol[c];
+        pmax = pmin = p;
+        umax = sqrt(w[3] * w[3] + w[4] * w[4] + w[5] * w[5]);
+    }
+    sh[0][threadIdx.x] = vv;
+    sh[1][threadIdx.x] = pmax;
+    sh[2][threadIdx.x] = pmin;
+    sh[3][threadIdx.x] = umax;
+    __syncthreads();
+    for (int st = kConsThreads / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) {
+            const int o = threadIdx.x + st;
+            sh[0][threadIdx.x] += sh[0][o];
+            sh[1][threadIdx.x] = fmax(sh[1][threadIdx.x], sh[1][o]);
+            sh[2][threadIdx.x] = fmin(sh[2][threadIdx.x], sh[2][o]);
+            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) blockOut[(size_t)blockIdx.x * 4 + threadIdx.x] = sh[threadIdx.x][0];
+}
+__global__ void k_probe_final(const double *blockOut, int nb, double *out) {
+    __shared__ double sh[4][1024];
+    double vv = 0.0, pmax = -1e300, pmin = 1e300, umax = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        vv += blockOut[(size_t)i * 4 + 0];
+        pmax = fmax(pmax, blockOut[(size_t)i * 4 + 1]);
+        pmin = fmin(pmin, blockOut[(size_t)i * 4 + 2]);
+        umax = fmax(umax, blockOut[(size_t)i * 4 + 3]);
+    }
+    sh[0][threadIdx.x] = vv;
+    sh[1][threadIdx.x] = pmax;
+    sh[2][threadIdx.x] = pmin;
+    sh[3][threadIdx.x] = umax;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) {
+            const int o = threadIdx.x + st;
+            sh[0][threadIdx.x] += sh[0][o];
+            sh[1][threadIdx.x] = fmax(sh[1][threadIdx.x], sh[1][o]);
+            sh[2][threadIdx.x] = fmin(sh[2][threadIdx.x], sh[2][o]);
+            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[threadIdx.x] = sh[threadIdx.x][0];
+}
+
 // ------------------------------------------------------------------ uploaded state check
 // firstBad = min over cells c of an AoS state Ua[c * 10 + v] that is not usable: a non-finite
 // sum, alpha outside [0, 1] (beyond 1e-9) or a negative partial density (the order-independent
@@ -623,8 +637,21 @@ __global__ void k_check_state(int n, const double *__restrict__ Ua, int32_t *fir
 }
 
 // ------------------------------------------------------------------ state layout conversion
-__global__ void k_scatter_state(int n, const double *__restrict__ Ua, const int32_t *__restrict__ new2old, double *U) {
+// U (renumbered SoA) = the uploaded AoS state, unless the check found an unusable cell: then U is
+// left as it was and flags[1] = that cell + 1.  A state that replaces U clears both flags (the
+// RK kernels' flags[0] and a previous rejection).
+__global__ void k_scatter_state(int n, const double *__restrict__ Ua, const int32_t *__restrict__ new2old, double *U,
+                                const int32_t *firstBad, int32_t *flags) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int fb = *firstBad;
+    if (fb < n) {
+        if (c == 0) flags[1] = fb + 1;
+        return;
+    }
+    if (c == 0) {
+        flags[0] = 0;
+        flags[1] = 0;
+    }
     if (c >= n) return;
     const size_t o = (size_t)new2old[c] * NV;
 #pragma unroll
@@ -644,23 +671,26 @@ __global__ void k_copy(size_t cnt, const double *__restrict__ a, double *b) {
 }
 
 // ------------------------------------------------------------------ halo records (partitioned runs)
-// out[k * stride + v] = rec[cells[k] * stride + v]: the records of the cells another part needs
+// out[k * nval + v] = value v of the record of cells[k] (records of nRec cells, nval values each):
+// the records of the cells another part needs, packed whole
 template <typename T>
-__global__ void k_halo_pack(const T *__restrict__ rec, int stride, const int32_t *__restrict__ cells, int cnt,
-                            T *__restrict__ out) {
+__global__ void k_halo_pack(const T *__restrict__ rec, size_t nRec, int nval, const int32_t *__restrict__ cells,
+                            int cnt, T *__restrict__ out) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)cnt * stride) return;
-    const size_t k = i / stride, v = i - k * stride;
-    out[i] = rec[(size_t)cells[k] * stride + v];
+    if (i >= (size_t)cnt * nval) return;
+    const size_t k = i / nval;
+    const int v = (int)(i - k * nval);
+    out[i] = rec[rec_index<T>(nRec, (size_t)cells[k], v)];
 }
-// rec[cells[k] * stride + v] = in[k * stride + v]: the ghosts' records received from their parts
+// value v of the record of cells[k] = in[k * nval + v]: the ghosts' records received from their parts
 template <typename T>
-__global__ void k_halo_unpack(T *__restrict__ rec, int stride, const int32_t *__restrict__ cells, int cnt,
+__global__ void k_halo_unpack(T *__restrict__ rec, size_t nRec, int nval, const int32_t *__restrict__ cells, int cnt,
                               const T *__restrict__ in) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)cnt * stride) return;
-    const size_t k = i / stride, v = i - k * stride;
-    rec[(size_t)cells[k] * stride + v] = in[i];
+    if (i >= (size_t)cnt * nval) return;
+    const size_t k = i / nval;
+    const int v = (int)(i - k * nval);
+    rec[rec_index<T>(nRec, (size_t)cells[k], v)] = in[i];
 }
 
 // ------------------------------------------------------------------ launchers
@@ -714,22 +744,22 @@ void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, Stag
     k_update<T><<<(m.nU + 255) / 256, 256, 0, s>>>(m, f, D, sc);
 }
 template <typename T>
-void launch_halo_pack(const T *rec, int stride, const int32_t *cells, int cnt, T *out, cudaStream_t s) {
-    const size_t tot = (size_t)cnt * stride;
-    if (tot) k_halo_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, stride, cells, cnt, out);
+void launch_halo_pack(const T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, T *out, cudaStream_t s) {
+    const size_t tot = (size_t)cnt * nval;
+    if (tot) k_halo_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, nRec, nval, cells, cnt, out);
 }
 template <typename T>
-void launch_halo_unpack(T *rec, int stride, const int32_t *cells, int cnt, const T *in, cudaStream_t s) {
-    const size_t tot = (size_t)cnt * stride;
-    if (tot) k_halo_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, stride, cells, cnt, in);
+void launch_halo_unpack(T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, const T *in, cudaStream_t s) {
+    const size_t tot = (size_t)cnt * nval;
+    if (tot) k_halo_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, nRec, nval, cells, cnt, in);
 }
-template void launch_halo_pack<float>(const float *, int, const int32_t *, int, float *, cudaStream_t);
-template void launch_halo_pack<double>(const double *, int, const int32_t *, int, double *, cudaStream_t);
-template void launch_halo_unpack<float>(float *, int, const int32_t *, int, const float *, cudaStream_t);
-template void launch_halo_unpack<double>(double *, int, const int32_t *, int, const double *, cudaStream_t);
+template void launch_halo_pack<float>(const float *, size_t, int, const int32_t *, int, float *, cudaStream_t);
+template void launch_halo_pack<double>(const double *, size_t, int, const int32_t *, int, double *, cudaStream_t);
+template void launch_halo_unpack<float>(float *, size_t, int, const int32_t *, int, const float *, cudaStream_t);
+template void launch_halo_unpack<double>(double *, size_t, int, const int32_t *, int, const double *, cudaStream_t);
 template <typename T>
-void launch_prim(int n, const double *U, T *W, const PhysD &D, cudaStream_t s) {
-    k_prim<T><<<(n + 255) / 256, 256, 0, s>>>(n, U, W, D);
+void launch_prim(int n, const double *U, T *W, size_t wStride, const PhysD &D, cudaStream_t s) {
+    k_prim<T><<<(n + 255) / 256, 256, 0, s>>>(n, U, W, wStride, D);
 }
 void launch_dt_finalize(const double *blockMin, int nBlocks, double cfl, double maxDt, double *dt, cudaStream_t s) {
     k_dt_finalize<<<1, 1024, 0, s>>>(blockMin, nBlocks, cfl, maxDt, dt);
@@ -739,13 +769,20 @@ void launch_cons(int n, int ivar, const double *U, const double *vol, double *bl
     k_cons_blocks<<<nb, kConsThreads, 0, s>>>(n, ivar, U, vol, blockSum);
     k_cons_final<<<1, 1024, 0, s>>>(blockSum, nb, out);
 }
+void launch_probe(int n, const double *U, const double *vol, const PhysD &D, double *blockOut, double *out,
+                  cudaStream_t s) {
+    const int nb = cons_blocks(n);
+    k_probe_blocks<<<nb, kConsThreads, 0, s>>>(n, U, vol, D, blockOut);
+    k_probe_final<<<1, 1024, 0, s>>>(blockOut, nb, out);
+}
 void launch_check_state(int n, const double *Ua, int32_t *firstBad, cudaStream_t s) {
-    static const int32_t none = INT_MAX;
-    cudaMemcpyAsync(firstBad, &none, sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    // "none" = 0x7f7f7f7f, above any cell count
+    cudaMemsetAsync(firstBad, 0x7f, sizeof(int32_t), s);
     if (n > 0) k_check_state<<<(n + 255) / 256, 256, 0, s>>>(n, Ua, firstBad);
 }
-void launch_scatter_state(int n, const double *Ua, const int32_t *new2old, double *U, cudaStream_t s) {
-    k_scatter_state<<<(n + 255) / 256, 256, 0, s>>>(n, Ua, new2old, U);
+void launch_scatter_state(int n, const double *Ua, const int32_t *new2old, double *U, const int32_t *firstBad,
+                          int32_t *flags, cudaStream_t s) {
+    k_scatter_state<<<(n + 255) / 256, 256, 0, s>>>(n, Ua, new2old, U, firstBad, flags);
 }
 void launch_gather_state(int n, const double *U, const int32_t *new2old, double *Ua, cudaStream_t s) {
     k_gather_state<<<(n + 255) / 256, 256, 0, s>>>(n, U, new2old, Ua);
@@ -763,7 +800,7 @@ template void launch_gather<float>(const DevMesh<float> &, const Fields<float> &
 template void launch_gather<double>(const DevMesh<double> &, const Fields<double> &, const PhysD &, int, int, StageCoef, cudaStream_t);
 template void launch_update<float>(const DevMesh<float> &, const Fields<float> &, const PhysD &, StageCoef, cudaStream_t);
 template void launch_update<double>(const DevMesh<double> &, const Fields<double> &, const PhysD &, StageCoef, cudaStream_t);
-template void launch_prim<float>(int, const double *, float *, const PhysD &, cudaStream_t);
-template void launch_prim<double>(int, const double *, double *, const PhysD &, cudaStream_t);
+template void launch_prim<float>(int, const double *, float *, size_t, const PhysD &, cudaStream_t);
+template void launch_prim<double>(int, const double *, double *, size_t, const PhysD &, cudaStream_t);
 
 }  // namespace fg

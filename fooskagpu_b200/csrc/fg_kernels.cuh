@@ -69,8 +69,17 @@ constexpr int FREC = 12;
 #ifndef FG_GATHER_THREADS
 #define FG_GATHER_THREADS 128
 #endif
+#ifndef FG_GRAD_MINB
+#define FG_GRAD_MINB 6
+#endif
+#ifndef FG_FACE_MINB
+#define FG_FACE_MINB (6 * 128 / FG_FACE_THREADS)
+#endif
+#ifndef FG_GATHER_MINB
+#define FG_GATHER_MINB (5 * 256 / FG_GATHER_THREADS)
+#endif
 template <typename T> struct MinBlocks {
-    static constexpr int grad = 6, face = 6 * 128 / FG_FACE_THREADS, gather = 5 * 256 / FG_GATHER_THREADS;
+    static constexpr int grad = FG_GRAD_MINB, face = FG_FACE_MINB, gather = FG_GATHER_MINB;
 };
 template <> struct MinBlocks<double> { static constexpr int grad = 0, face = 0, gather = 0; };
 template <typename T> struct StageCells { static constexpr int value = FG_STAGE_CELLS_F; };
@@ -82,9 +91,9 @@ struct Fields {
     double *U;          // [10][n]
     double *U0;         // [10][n]
     double *RHS;        // [10][n] (RHS-mode residual)
-    T *Win;             // [n][WREC] primitive record read this stage
-    T *Wout;            // [n][WREC] primitive record written this stage
-    T *G;               // [n][GREC] limiter + gradient
+    T *Win;             // primitive records (WREC values per cell, component-major) read this stage
+    T *Wout;            // primitive records written this stage
+    T *G;               // limiter + gradient records (GREC values per cell, component-major)
     double *signal;     // [n]
     double *blockMin;   // [nBlocks]
     double *dt;         // device scalar
@@ -123,13 +132,15 @@ void launch_gather(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, int 
                    StageCoef sc, cudaStream_t s);
 template <typename T>
 void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, StageCoef sc, cudaStream_t s);
+// primitive records of the first n cells from U (records of wStride cells)
 template <typename T>
-void launch_prim(int n, const double *U, T *W, const PhysD &D, cudaStream_t s);
-// partitioned runs: records (stride values each) of cells[0..cnt) to / from a contiguous buffer
+void launch_prim(int n, const double *U, T *W, size_t wStride, const PhysD &D, cudaStream_t s);
+// partitioned runs: the records (nval values each, records of nRec cells) of cells[0..cnt) to /
+// from a contiguous buffer of whole records
 template <typename T>
-void launch_halo_pack(const T *rec, int stride, const int32_t *cells, int cnt, T *out, cudaStream_t s);
+void launch_halo_pack(const T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, T *out, cudaStream_t s);
 template <typename T>
-void launch_halo_unpack(T *rec, int stride, const int32_t *cells, int cnt, const T *in, cudaStream_t s);
+void launch_halo_unpack(T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, const T *in, cudaStream_t s);
 // dt = min(cfl * min_blocks, maxDt) from blockMin[nBlocks]
 void launch_dt_finalize(const double *blockMin, int nBlocks, double cfl, double maxDt, double *dt, cudaStream_t s);
 int flux_blocks(int n);   // blocks of the gather kernel (= entries of blockMin)
@@ -162,17 +173,23 @@ struct RelaxOrder {
 int relax_order_blocks(int n);
 // returns the number of kernels launched
 template <typename T>
-int launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
+int launch_relax(int n, double *U, T *W, size_t wStride, const PhysD &D, const RelaxParams &R, int32_t *counters,
                  const SurrogateDev &S, const RelaxLog &L, const RelaxOrder &O, cudaStream_t s);
 
 // conservation integral: blockSum then ordered final sum into out
 void launch_cons(int n, int ivar, const double *U, const double *vol, double *blockSum, double *out, cudaStream_t s);
 int cons_blocks(int n);
+// state probe: out[4] = vapour volume, max / min mixture pressure, max speed (blockOut: 4 per
+// cons_blocks(n) block)
+void launch_probe(int n, const double *U, const double *vol, const PhysD &D, double *blockOut, double *out,
+                  cudaStream_t s);
 
-// first cell of an uploaded AoS state (n x 10) that is not usable, INT_MAX if none
+// first cell of an uploaded AoS state (n x 10) that is not usable, 0x7f7f7f7f if none
 void launch_check_state(int n, const double *Uaos, int32_t *firstBad, cudaStream_t s);
 // reference-order AoS <-> renumbered SoA
-void launch_scatter_state(int n, const double *Uaos, const int32_t *new2old, double *U, cudaStream_t s);
+// scatter unless firstBad (set by launch_check_state) names a cell: see k_scatter_state for flags
+void launch_scatter_state(int n, const double *Uaos, const int32_t *new2old, double *U, const int32_t *firstBad,
+                          int32_t *flags, cudaStream_t s);
 void launch_gather_state(int n, const double *U, const int32_t *new2old, double *Uaos, cudaStream_t s);
 void launch_copy_u0(int n, const double *U, double *U0, cudaStream_t s);
 

@@ -126,6 +126,39 @@ const char kBcs[] = "BOUNDARY CONDITIONS ";
 
 }  // namespace
 
+// Cell centres, per-element face centres and element-type counts from the element lists.
+static void finish_elements(Mesh &m) {
+    const size_t elnum = (size_t)m.nElem;
+    m.cellCenter.assign(elnum * 3, 0.0);
+    m.elFcCenter.assign(elnum * 18, 0.0);
+    m.nTet = m.nPyr = m.nPrism = m.nHex = 0;
+    for (size_t e = 0; e < elnum; e++) {
+        const int nc = m.elNN[e];
+        const ElemType *et = elem_type_for_nodes(nc);
+        // cell centre: plain average in node order (DP/translator.cu:138-143, 183-188, 223-228, 261-263)
+        for (int d = 0; d < 3; d++) {
+            double sum = m.nodes[(size_t)m.elNodes[e * 8 + 0] * 3 + d];
+            for (int k = 1; k < nc; k++) sum = sum + m.nodes[(size_t)m.elNodes[e * 8 + k] * 3 + d];
+            m.cellCenter[e * 3 + d] = sum / nc;
+        }
+        // face centres in the reference's node order
+        for (int f = 0; f < et->nFaces; f++) {
+            const int cnt = et->faceNodeCount[f];
+            for (int d = 0; d < 3; d++) {
+                double sum = m.nodes[(size_t)m.elNodes[e * 8 + et->centreNodes[f][0]] * 3 + d];
+                for (int k = 1; k < cnt; k++) sum = sum + m.nodes[(size_t)m.elNodes[e * 8 + et->centreNodes[f][k]] * 3 + d];
+                m.elFcCenter[e * 18 + f * 3 + d] = sum / cnt;
+            }
+        }
+        switch (nc) {
+        case 4: m.nTet++; break;
+        case 5: m.nPyr++; break;
+        case 6: m.nPrism++; break;
+        default: m.nHex++; break;
+        }
+    }
+}
+
 int read_neu(const std::string &path, double scale, Mesh &m, std::string &err) {
     FILE *fp = fopen(path.c_str(), "rb");
     if (!fp) {
@@ -181,8 +214,6 @@ int read_neu(const std::string &path, double scale, Mesh &m, std::string &err) {
     m.elNodes.assign((size_t)elnum * 8, 0);
     m.elNN.assign(elnum, 0);
     m.elBc.assign((size_t)elnum * 6, 0);
-    m.cellCenter.assign((size_t)elnum * 3, 0.0);
-    m.elFcCenter.assign((size_t)elnum * 18, 0.0);
     std::vector<char> seen(elnum, 0);
     for (long i = 0; i < elnum; i++) {
         long el, typ, nc;
@@ -202,30 +233,10 @@ int read_neu(const std::string &path, double scale, Mesh &m, std::string &err) {
             m.elNodes[e * 8 + k] = (int32_t)(c - 1);
         }
         m.elNN[e] = (int32_t)nc;
-        // cell centre: plain average in node order (DP/translator.cu:138-143, 183-188, 223-228, 261-263)
-        for (int d = 0; d < 3; d++) {
-            double sum = m.nodes[(size_t)m.elNodes[e * 8 + 0] * 3 + d];
-            for (int k = 1; k < nc; k++) sum = sum + m.nodes[(size_t)m.elNodes[e * 8 + k] * 3 + d];
-            m.cellCenter[e * 3 + d] = sum / nc;
-        }
-        // face centres in the reference's node order
-        for (int f = 0; f < et->nFaces; f++) {
-            const int cnt = et->faceNodeCount[f];
-            for (int d = 0; d < 3; d++) {
-                double sum = m.nodes[(size_t)m.elNodes[e * 8 + et->centreNodes[f][0]] * 3 + d];
-                for (int k = 1; k < cnt; k++) sum = sum + m.nodes[(size_t)m.elNodes[e * 8 + et->centreNodes[f][k]] * 3 + d];
-                m.elFcCenter[e * 18 + f * 3 + d] = sum / cnt;
-            }
-        }
-        switch (nc) {
-        case 4: m.nTet++; break;
-        case 5: m.nPyr++; break;
-        case 6: m.nPrism++; break;
-        default: m.nHex++; break;
-        }
     }
     if (!r.seek_section(kBcs)) {
         if (bcnum > 0) { err = "no BOUNDARY CONDITIONS section"; return FG_ERR_MESH; }
+        finish_elements(m);
         return FG_OK;
     }
     for (long b = 0; b < bcnum; b++) {
@@ -256,6 +267,40 @@ int read_neu(const std::string &path, double scale, Mesh &m, std::string &err) {
     }
     for (long e = 0; e < elnum; e++)
         if (!seen[e]) { err = "element " + std::to_string(e + 1) + " missing"; return FG_ERR_MESH; }
+    finish_elements(m);
+    return FG_OK;
+}
+
+int mesh_from_arrays(int nNodes, const double *nodes, int nElem, const int32_t *elNN, const int32_t *elNodes,
+                     const int32_t *elBc, double scale, Mesh &m, std::string &err) {
+    if (nNodes <= 0 || nElem <= 0 || nElem > (1 << 28)) { err = "node / element counts out of range"; return FG_ERR_ARG; }
+    m.nNodes = nNodes;
+    m.nElem = nElem;
+    m.nodes.resize((size_t)nNodes * 3);
+    for (size_t i = 0; i < (size_t)nNodes * 3; i++) m.nodes[i] = nodes[i] * scale;
+    m.elNodes.assign((size_t)nElem * 8, 0);
+    m.elNN.assign(nElem, 0);
+    m.elBc.assign((size_t)nElem * 6, 0);
+    for (size_t e = 0; e < (size_t)nElem; e++) {
+        const int nc = elNN[e];
+        const ElemType *et = elem_type_for_nodes(nc);
+        if (!et) { err = "unsupported element with " + std::to_string(nc) + " nodes at " + std::to_string(e); return FG_ERR_MESH; }
+        m.elNN[e] = nc;
+        for (int k = 0; k < nc; k++) {
+            const int32_t c = elNodes[e * 8 + k];
+            if (c < 0 || c >= nNodes) { err = "node id out of range in element " + std::to_string(e); return FG_ERR_MESH; }
+            m.elNodes[e * 8 + k] = c;
+        }
+        for (int f = 0; f < 6; f++) {
+            const int32_t bc = elBc[e * 6 + f];
+            if (bc < 0 || bc > 5 || (bc != 0 && f >= et->nFaces)) {
+                err = "boundary code out of range at element " + std::to_string(e) + " face " + std::to_string(f);
+                return FG_ERR_MESH;
+            }
+            m.elBc[e * 6 + f] = bc;
+        }
+    }
+    finish_elements(m);
     return FG_OK;
 }
 

@@ -54,6 +54,10 @@ struct Mesh {
 // Parse a Gambit neutral file with the reference's grammar (DP/translator.cu:3-354).
 // Returns FG_OK or an error code with a message in err.
 int read_neu(const std::string &path, double scale, Mesh &m, std::string &err);
+// The same element lists handed over in memory: nodes[nNodes*3] (multiplied by scale),
+// elNN[nElem], elNodes[nElem*8] (0-based), elBc[nElem*6] (internal codes 0..5).
+int mesh_from_arrays(int nNodes, const double *nodes, int nElem, const int32_t *elNN, const int32_t *elNodes,
+                     const int32_t *elBc, double scale, Mesh &m, std::string &err);
 // Match faces, build the reference face order and geometry, renumber (host).
 int finish_mesh(Mesh &m, const fg_mesh_opts &o, std::string &err);
 // The same on the GPU (o.device); identical arrays.

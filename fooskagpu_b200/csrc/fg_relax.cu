@@ -471,7 +471,7 @@ struct InRelax {
 #define FG_CHEM_MINBLOCKS 4
 #endif
 template <typename T, bool kSG, bool kLog, bool kOrd>
-__global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBLOCKS) k_relax(int n, double *U, T *W, const PhysD D, const RelaxParams R,
+__global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBLOCKS) k_relax(int n, double *U, T *W, size_t wStride, const PhysD D, const RelaxParams R,
                                                int32_t *counters, const SurrogateDev S, const RelaxLog Lg,
                                                const int32_t *order, const int32_t *nChem, const float4 *pred,
                                                const int32_t *hullOk) {
@@ -531,11 +531,7 @@ __global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBL
         U[(size_t)9 * n + c] = u[9];
         T w[NP];
         cons2prim_d(D, u, w);
-        T *p = W + (size_t)c * WREC;
-#pragma unroll
-        for (int v = 0; v < NP; v++) p[v] = w[v];
-#pragma unroll
-        for (int v = NP; v < WREC; v++) p[v] = 0;
+        rec_store<T, NP>(W, wStride, c, w);
     }
     // warp-aggregated counters (sums of integers: order does not matter)
     const unsigned mask = __ballot_sync(0xffffffffu, act && chem);
@@ -557,7 +553,7 @@ __global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBL
 int relax_order_blocks(int n) { return (n + kOrdThreads - 1) / kOrdThreads; }
 
 template <typename T, bool kOrd>
-static void launch_relax_k(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
+static void launch_relax_k(int n, double *U, T *W, size_t wStride, const PhysD &D, const RelaxParams &R, int32_t *counters,
                            const SurrogateDev &S, const RelaxLog &L, const RelaxOrder *O, cudaStream_t s) {
     const int nb = (n + 127) / 128;
     const bool lg = L.count != nullptr;
@@ -565,21 +561,21 @@ static void launch_relax_k(int n, double *U, T *W, const PhysD &D, const RelaxPa
     const float4 *pred = O ? O->pred : nullptr;
     const int32_t *hull = O ? O->hullOk : nullptr;
     if (kOrd && S.enabled && lg)
-        k_relax<T, true, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem, pred, hull);
+        k_relax<T, true, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
     else if (kOrd && S.enabled)
-        k_relax<T, true, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem, pred, hull);
+        k_relax<T, true, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
     else if (lg)
-        k_relax<T, false, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem, pred, hull);
+        k_relax<T, false, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
     else
-        k_relax<T, false, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, D, R, counters, S, L, order, nChem, pred, hull);
+        k_relax<T, false, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
 }
 
 template <typename T>
-int launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, int32_t *counters,
+int launch_relax(int n, double *U, T *W, size_t wStride, const PhysD &D, const RelaxParams &R, int32_t *counters,
                  const SurrogateDev &S, const RelaxLog &L, const RelaxOrder &O, cudaStream_t s) {
     if (R.chemFlag != 1) {
         // every cell is thermal: no ordering needed (and no surrogate)
-        launch_relax_k<T, false>(n, U, W, D, R, counters, SurrogateDev{}, L, nullptr, s);
+        launch_relax_k<T, false>(n, U, W, wStride, D, R, counters, SurrogateDev{}, L, nullptr, s);
         return 1;
     }
     const int nb = relax_order_blocks(n);
@@ -594,13 +590,13 @@ int launch_relax(int n, double *U, T *W, const PhysD &D, const RelaxParams &R, i
                                                                         O.pred, O.hullOk, O.tcErr);
         k++;
     }
-    launch_relax_k<T, true>(n, U, W, D, R, counters, S, L, &O, s);
+    launch_relax_k<T, true>(n, U, W, wStride, D, R, counters, S, L, &O, s);
     return k;
 }
 
-template int launch_relax<float>(int, double *, float *, const PhysD &, const RelaxParams &, int32_t *,
+template int launch_relax<float>(int, double *, float *, size_t, const PhysD &, const RelaxParams &, int32_t *,
                                  const SurrogateDev &, const RelaxLog &, const RelaxOrder &, cudaStream_t);
-template int launch_relax<double>(int, double *, double *, const PhysD &, const RelaxParams &, int32_t *,
+template int launch_relax<double>(int, double *, double *, size_t, const PhysD &, const RelaxParams &, int32_t *,
                                   const SurrogateDev &, const RelaxLog &, const RelaxOrder &, cudaStream_t);
 
 }  // namespace fg

@@ -74,12 +74,20 @@ struct fg_solver {
     }
     int init_flag() {
         void *h = nullptr;
-        FG_CUDA_TRY(cudaHostAlloc(&h, sizeof(int32_t), cudaHostAllocMapped));
+        FG_CUDA_TRY(cudaHostAlloc(&h, 2 * sizeof(int32_t), cudaHostAllocMapped));
         hBad = static_cast<volatile int32_t *>(h);
-        *hBad = 0;
+        hBad[0] = 0;
+        hBad[1] = 0;
         FG_CUDA_TRY(cudaHostGetDevicePointer((void **)&dBad, h, 0));
         return FG_OK;
     }
+    int upload_error() const {
+        return set_err(FG_ERR_NAN, "fg_set_state: cell " + std::to_string(hBad[1] - 1) +
+                                       " is not finite or has alpha outside [0, 1] or a negative partial density"
+                                       " (the state was not replaced)");
+    }
+    // a flagged state (RK kernels) or a rejected upload, in that order of precedence
+    int flag_error() const { return hBad[1] ? upload_error() : bad_state_error(); }
     int bad_state_error() const {
         return set_err(FG_ERR_NAN, "the state became non-finite or its density non-positive in step " +
                                        std::to_string(*hBad - 1) + " (reset it with fg_set_state / fg_checkpoint_read)");
@@ -127,7 +135,8 @@ struct fg_solver {
     }
     fg_case cs{};
     int precision = FG_PREC_FP64;
-    // failure flag written by the RK kernels (mapped host memory: read without a stream sync)
+    // failure flags (mapped host memory: read without a stream sync): [0] step + 1 of a state the
+    // RK kernels found unusable, [1] first unusable cell + 1 of a rejected upload
     volatile int32_t *hBad = nullptr;
     int32_t *dBad = nullptr;
     std::vector<double> cellCenter;   // reference order, for the field dump
@@ -169,7 +178,9 @@ struct fg_solver {
         if (halo.allreduce(halo.ctx, op, v) != 0) return set_err(FG_ERR_CUDA, "partitioned run: allreduce failed");
         return FG_OK;
     }
-    virtual int set_state(const double *U, cudaStream_t s) = 0;
+    // upload U; wait = true synchronises and reports a rejected upload, false leaves the report to
+    // the flags (fg_step / fg_check_state)
+    virtual int set_state(const double *U, cudaStream_t s, bool wait) = 0;
     virtual int get_state(double *U, cudaStream_t s) = 0;
     virtual int compute_rhs(int wantSignal, cudaStream_t s) = 0;
     virtual int time_step(double *dtOut, cudaStream_t s) = 0;
@@ -179,6 +190,7 @@ struct fg_solver {
     virtual int relax(fg_relax_stats *st, cudaStream_t s) = 0;
     virtual int relax_counts(fg_relax_stats *st) = 0;
     virtual int cons(int ivar, double *out, cudaStream_t s) = 0;
+    virtual int probe(double *out4, cudaStream_t s) = 0;
     virtual int advance_time(cudaStream_t s) = 0;
     virtual int get_time(double *dt, double *t) = 0;
     virtual int set_dt(double dt) = 0;
@@ -198,8 +210,8 @@ __global__ void k_advance_time(const double *dt, double *t) { *t += *dt; }
 // rho U V W pressure temperature vaporMass |grad rho|, the last from the most recent gradient
 // pass; written to out[old * 13 + k] (the .neu element order)
 template <typename T>
-__global__ void k_field_vars(int n, const double *__restrict__ U, const T *__restrict__ G, const int32_t *new2old,
-                             const PhysD D, const double *cp, double *out) {
+__global__ void k_field_vars(int n, const double *__restrict__ U, const T *__restrict__ G, size_t gStride,
+                             const int32_t *new2old, const PhysD D, const double *cp, double *out) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     double u[NV];
@@ -214,10 +226,11 @@ __global__ void k_field_vars(int n, const double *__restrict__ U, const T *__res
     const double tL = (pL + D.pinf[0]) / ((cp[0] / D.gam[0]) * D.gm1[0] * rL);
     const double tG = (pG + D.pinf[1]) / ((cp[1] / D.gam[1]) * D.gm1[1] * rG);
     // grad rho = (rhoL - rhoG) grad alpha + alpha grad rhoL + (1 - alpha) grad rhoG
-    const T *g = G + (size_t)c * GREC + NP;   // gradients of W: var v at g[3 v + d]
+    // gradients of W: component d of var v is value NP + 3 v + d of the record
+    auto g = [&](int q) { return (double)G[rec_index<T>(gStride, (size_t)c, NP + q)]; };
     double gr[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) gr[d] = (rL - rG) * (double)g[d] + aL * (double)g[3 + d] + aG * (double)g[6 + d];
+    for (int d = 0; d < 3; d++) gr[d] = (rL - rG) * g(d) + aL * g(3 + d) + aG * g(6 + d);
     double *o = out + (size_t)new2old[c] * 13;
     o[3] = aL;
     o[4] = aG;
@@ -240,6 +253,7 @@ struct SolverT : public fg_solver {
     DevBuf dPred, dHullOk, dTcErr;                          // surrogate predictions
     DevBuf dSendCells, dRecvCells;                          // halo lists of a partitioned mesh
     DevBuf dChk;                                            // set_state: first unusable cell
+    DevBuf dProbe;                                          // fg_probe block results (on first use)
     std::vector<int32_t> sendStart, recvStart;
     int cur = 0;
     DevMesh<T> dm{};
@@ -313,8 +327,10 @@ struct SolverT : public fg_solver {
         P.energyFix = (cs.hllcEnergyFix == 1);
         P.tieTol = (T)cs.hllcTieTol;
         {
-            // inlet ghost (DP/bc.h:2-25): rho from p = 11.4e5 Pa, T = 115.3 K
-            const double pIn = 11.4e5, tIn = 115.3;
+            // inlet ghost (DP/bc.h:2-25): rho from p = 11.4e5 Pa, T = 115.3 K, or the case's
+            // prescribed inlet state (extension)
+            const bool own = (cs.inletStateFlag == 1);
+            const double pIn = own ? cs.inletP : 11.4e5, tIn = own ? cs.inletT : 115.3;
             P.inAlpha = (T)(1.0 - cs.avfMin);
             P.inRhoL = (T)((pIn + cs.pInf[0]) / ((cs.Cp[0] / cs.gamma[0]) * tIn * (cs.gamma[0] - 1)));
             P.inRhoG = (T)((pIn + cs.pInf[1]) / ((cs.Cp[1] / cs.gamma[1]) * tIn * (cs.gamma[1] - 1)));
@@ -591,28 +607,28 @@ struct SolverT : public fg_solver {
         return FG_OK;
     }
 
-    int set_state(const double *U, cudaStream_t s) override {
-        FG_CUDA_TRY(cudaStreamSynchronize(s));
+    int set_state(const double *U, cudaStream_t s, bool wait) override {
         FG_CUDA_TRY(cudaMemcpyAsync(dStage.p, U, (size_t)nU * NV * sizeof(double), cudaMemcpyHostToDevice, s));
-        // checked on the device before it replaces the state (only the staging buffer so far)
+        // checked on the device; the scatter replaces the state only if every cell is usable
         prof_begin(FG_K_OTHER, s);
         launch_check_state(nU, dStage.as<double>(), dChk.as<int32_t>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("set_state check");
-        int32_t bad = 0;
-        FG_CUDA_TRY(cudaMemcpyAsync(&bad, dChk.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        FG_CUDA_TRY(cudaStreamSynchronize(s));
-        if (bad != INT_MAX)
-            return set_err(FG_ERR_NAN, "fg_set_state: cell " + std::to_string(bad) +
-                                           " is not finite or has alpha outside [0, 1] or a negative partial density");
-        *hBad = 0;
         prof_begin(FG_K_OTHER, s);
-        launch_scatter_state(nU, dStage.as<double>(), dNew2Old.as<int32_t>(), dU.as<double>(), s);
+        launch_scatter_state(nU, dStage.as<double>(), dNew2Old.as<int32_t>(), dU.as<double>(), dChk.as<int32_t>(),
+                             dBad, s);
         prof_end(s);
         prof_begin(FG_K_OTHER, s);
-        launch_prim<T>(nU, dU.as<double>(), dW[cur].as<T>(), D, s);
+        launch_prim<T>(nU, dU.as<double>(), dW[cur].as<T>(), (size_t)n, D, s);
         prof_end(s);
         FG_LAUNCH_CHECK("set_state");
+        if (!wait) return FG_OK;
+        FG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (hBad[1]) {
+            const int rc = upload_error();
+            hBad[1] = 0;   // reported here: the old state stays usable
+            return rc;
+        }
         return FG_OK;
     }
     int get_state(double *U, cudaStream_t s) override {
@@ -659,14 +675,14 @@ struct SolverT : public fg_solver {
         const int stride = (field == FG_HALO_W) ? WREC : GREC;
         const int nSend = sendStart.back(), nRecv = recvStart.back();
         prof_begin(FG_K_OTHER, s);
-        launch_halo_pack<T>(rec, stride, dSendCells.as<int32_t>(), nSend, static_cast<T *>(haloSend), s);
+        launch_halo_pack<T>(rec, (size_t)n, stride, dSendCells.as<int32_t>(), nSend, static_cast<T *>(haloSend), s);
         prof_end(s);
         FG_LAUNCH_CHECK("halo pack");
         FG_CUDA_TRY(cudaStreamSynchronize(s));
         if (halo.exchange(halo.ctx, field, (int64_t)stride * (int64_t)sizeof(T), s) != 0)
             return set_err(FG_ERR_CUDA, "partitioned run: halo exchange failed");
         prof_begin(FG_K_OTHER, s);
-        launch_halo_unpack<T>(rec, stride, dRecvCells.as<int32_t>(), nRecv, static_cast<const T *>(haloRecv), s);
+        launch_halo_unpack<T>(rec, (size_t)n, stride, dRecvCells.as<int32_t>(), nRecv, static_cast<const T *>(haloRecv), s);
         prof_end(s);
         FG_LAUNCH_CHECK("halo unpack");
         return FG_OK;
@@ -738,7 +754,7 @@ struct SolverT : public fg_solver {
         const RelaxOrder O{dOrdFlag.as<uint8_t>(), dOrdCnt.as<int32_t>(), dOrdOff.as<int32_t>(), dOrder.as<int32_t>(),
                            dOrdTotal.as<int32_t>(), dPred.as<float4>(), dHullOk.as<int32_t>(), dTcErr.as<int32_t>()};
         prof_begin(FG_K_RELAX, s);
-        const int k = launch_relax<T>(nU, dU.as<double>(), dW[cur].as<T>(), D, R, dCnt.as<int32_t>(), S, L, O, s);
+        const int k = launch_relax<T>(nU, dU.as<double>(), dW[cur].as<T>(), (size_t)n, D, R, dCnt.as<int32_t>(), S, L, O, s);
         prof_end(s);
         launches += k - 1;
         FG_LAUNCH_CHECK("relaxation");
@@ -758,6 +774,22 @@ struct SolverT : public fg_solver {
         st->nIter = h[3];
         st->nSurrogate = h[4];
         st->nFallback = h[5];
+        return FG_OK;
+    }
+    int probe(double *out4, cudaStream_t s) override {
+        if (parted) return set_err(FG_ERR_UNSUPPORTED, "fg_probe: not available on a part of a partitioned mesh");
+        if (!dProbe.p) {
+            FG_CUDA_TRY(dProbe.alloc(((size_t)4 * cons_blocks(nU) + 4) * sizeof(double)));
+            bytes += dProbe.bytes;
+        }
+        double *o = dProbe.as<double>() + (size_t)4 * cons_blocks(nU);
+        prof_begin(FG_K_OTHER, s);
+        launch_probe(nU, dU.as<double>(), dVol.as<double>(), D, dProbe.as<double>(), o, s);
+        prof_end(s);
+        launches++;  // two kernels
+        FG_LAUNCH_CHECK("probe");
+        FG_CUDA_TRY(cudaMemcpyAsync(out4, o, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        FG_CUDA_TRY(cudaStreamSynchronize(s));
         return FG_OK;
     }
     int cons(int ivar, double *out, cudaStream_t s) override {
@@ -815,7 +847,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dOut.alloc((size_t)nU * 13 * sizeof(double)));
         FG_CUDA_TRY(dCp.alloc(2 * sizeof(double)));
         FG_CUDA_TRY(cudaMemcpy(dCp.p, cs.Cp, 2 * sizeof(double), cudaMemcpyHostToDevice));
-        k_field_vars<T><<<(nU + 255) / 256, 256>>>(nU, dU.as<double>(), dG.as<T>(), dNew2Old.as<int32_t>(), D,
+        k_field_vars<T><<<(nU + 255) / 256, 256>>>(nU, dU.as<double>(), dG.as<T>(), (size_t)n, dNew2Old.as<int32_t>(), D,
                                                   dCp.as<double>(), dOut.as<double>());
         FG_LAUNCH_CHECK("field_vars");
         launches++;
@@ -831,16 +863,16 @@ struct SolverT : public fg_solver {
     }
     int get_limited(double *grad, double *theta) override {
         FG_CUDA_TRY(cudaDeviceSynchronize());
-        std::vector<T> g((size_t)nU * GREC);
+        std::vector<T> g((size_t)n * GREC);
         std::vector<int32_t> n2o(nU);
         FG_CUDA_TRY(cudaMemcpy(g.data(), dG.p, g.size() * sizeof(T), cudaMemcpyDeviceToHost));
         FG_CUDA_TRY(cudaMemcpy(n2o.data(), dNew2Old.p, (size_t)nU * sizeof(int32_t), cudaMemcpyDeviceToHost));
         for (int i = 0; i < nU; i++) {
             const size_t o = (size_t)n2o[i];
             for (int v = 0; v < NV; v++) {
-                if (theta) theta[o * NV + v] = (v < NP) ? (double)g[(size_t)i * GREC + v] : 0.0;
+                if (theta) theta[o * NV + v] = (v < NP) ? (double)g[rec_index<T>((size_t)n, i, v)] : 0.0;
                 for (int d = 0; d < 3; d++)
-                    if (grad) grad[(o * NV + v) * 3 + d] = (v < NP) ? (double)g[(size_t)i * GREC + NP + 3 * v + d] : 0.0;
+                    if (grad) grad[(o * NV + v) * 3 + d] = (v < NP) ? (double)g[rec_index<T>((size_t)n, i, NP + 3 * v + d)] : 0.0;
             }
         }
         return FG_OK;
@@ -931,6 +963,25 @@ int fg_mesh_load_neu(const char *path, const fg_mesh_opts *opts, fg_mesh **out) 
     std::unique_ptr<fg_mesh> m(new fg_mesh());
     std::string err;
     int rc = fg::read_neu(path, o.scale, m->m, err);
+    if (rc != FG_OK) return set_err(rc, err);
+    rc = o.gpu ? fg::finish_mesh_gpu(m->m, o, err) : fg::finish_mesh(m->m, o, err);
+    if (rc != FG_OK) return set_err(rc, err);
+    *out = m.release();
+    return FG_OK;
+}
+
+int fg_mesh_build(int32_t nNodes, const double *nodes, int32_t nElem, const int32_t *elNN, const int32_t *elNodes,
+                  const int32_t *elBc, const fg_mesh_opts *opts, fg_mesh **out) {
+    if (!nodes || !elNN || !elNodes || !elBc || !out) return set_err(FG_ERR_ARG, "fg_mesh_build: null argument");
+    *out = nullptr;
+    fg_mesh_opts o{};
+    o.scale = 1.0;
+    o.renumber = FG_RENUMBER_MORTON;
+    if (opts) o = *opts;
+    if (!(o.scale > 0)) return set_err(FG_ERR_ARG, "fg_mesh_build: scale must be > 0");
+    std::unique_ptr<fg_mesh> m(new fg_mesh());
+    std::string err;
+    int rc = fg::mesh_from_arrays(nNodes, nodes, nElem, elNN, elNodes, elBc, o.scale, m->m, err);
     if (rc != FG_OK) return set_err(rc, err);
     rc = o.gpu ? fg::finish_mesh_gpu(m->m, o, err) : fg::finish_mesh(m->m, o, err);
     if (rc != FG_OK) return set_err(rc, err);
@@ -1085,7 +1136,12 @@ int fg_solver_set_halo(fg_solver *s, const fg_halo_ops *ops, void *sendBuf, void
 int fg_set_state(fg_solver *s, const double *U, void *stream) {
     FG_ENTER(s);
     if (!U) return set_err(FG_ERR_ARG, "fg_set_state: null U");
-    return s->set_state(U, (cudaStream_t)stream);
+    return s->set_state(U, (cudaStream_t)stream, true);
+}
+int fg_set_state_async(fg_solver *s, const double *U, void *stream) {
+    FG_ENTER(s);
+    if (!U) return set_err(FG_ERR_ARG, "fg_set_state_async: null U");
+    return s->set_state(U, (cudaStream_t)stream, false);
 }
 int fg_get_state(fg_solver *s, double *U, void *stream) {
     FG_ENTER(s);
@@ -1177,6 +1233,19 @@ int fg_cons_calc(fg_solver *s, int32_t ivar, double *out, void *stream) {
     if (ivar < 0 || ivar >= 10) return set_err(FG_ERR_ARG, "ivar out of range");
     return s->cons(ivar, out, (cudaStream_t)stream);
 }
+int fg_probe(fg_solver *s, fg_probe_out *out, void *stream) {
+    FG_ENTER(s);
+    if (!out) return set_err(FG_ERR_ARG, "fg_probe: null output");
+    double v[4];
+    const int rc = s->probe(v, (cudaStream_t)stream);
+    if (rc != FG_OK) return rc;
+    out->vapourVolume = v[0];
+    out->maxPressure = v[1];
+    out->minPressure = v[2];
+    out->maxSpeed = v[3];
+    return FG_OK;
+}
+
 int fg_get_time(fg_solver *s, double *dt, double *physicalTime, int32_t *iStep) {
     FG_ENTER(s);
     if (iStep) *iStep = s->iStep;
@@ -1236,7 +1305,7 @@ int fg_checkpoint_read(fg_solver *s, const char *path) {
     ok = ok && fread(U.data(), sizeof(double), U.size(), fp) == U.size();
     fclose(fp);
     if (!ok) return set_err(FG_ERR_IO, std::string("fg_checkpoint_read: not a checkpoint or truncated: ") + path);
-    int rc = s->set_state(U.data(), 0);
+    int rc = s->set_state(U.data(), 0, true);
     if (rc == FG_OK) rc = s->set_dt(h.dt);
     if (rc == FG_OK) rc = s->set_time(h.physicalTime);
     if (rc != FG_OK) return rc;
@@ -1268,13 +1337,13 @@ int fg_field_dump(fg_solver *s, const char *path) {
 int fg_check_state(fg_solver *s, int32_t *badStep) {
     FG_ENTER(s);
     FG_CUDA_TRY(cudaDeviceSynchronize());
-    if (badStep) *badStep = *s->hBad ? *s->hBad - 1 : -1;
-    return *s->hBad ? s->bad_state_error() : FG_OK;
+    if (badStep) *badStep = s->hBad[0] ? s->hBad[0] - 1 : -1;
+    return (s->hBad[0] || s->hBad[1]) ? s->flag_error() : FG_OK;
 }
 
 int fg_step(fg_solver *s, void *stream) {
     FG_ENTER(s);
-    if (*s->hBad) return s->bad_state_error();
+    if (s->hBad[0] || s->hBad[1]) return s->flag_error();
     cudaStream_t st = (cudaStream_t)stream;
     const fg_case &c = s->cs;
     int rc = s->advance_time(st);   // physicalTime += dt (previous dt, DP/explicitLoop.cu:29)

@@ -118,8 +118,13 @@ typedef struct fg_case {
     /* inletVelFlag = 1: the inlet ghost (bc 3) takes the velocity inletVel instead of the
      * interior velocity (the reference's inlet copies it, DP/bc.h:8-18). */
     int32_t inletVelFlag;
-    int32_t reserved[3];
+    /* inletStateFlag = 1: the inlet ghost's phase densities and pressures come from inletP, inletT
+     * instead of the reference's fixed 11.4e5 Pa and 115.3 K (DP/bc.h:2-25). */
+    int32_t inletStateFlag;
+    int32_t reserved[2];
     double  inletVel[3];
+    double  inletP;
+    double  inletT;
 } fg_case;
 
 /* Fill *c with the values the reference hard-codes in DP/buildInput.cu:10-69. */
@@ -172,6 +177,15 @@ typedef struct fg_mesh_view {
 } fg_mesh_view;
 
 int  fg_mesh_load_neu(const char *path, const fg_mesh_opts *opts, fg_mesh **out);
+/* The same pipeline for element lists already in memory (a generator, another reader), without
+ * the text: what translator_ptw fills from the file (DP/translator.cu:24-349) handed over as
+ * arrays in .neu element order.  nodes[nNodes*3] (multiplied by opts->scale); elNN[nElem] nodes
+ * per element (4 tet, 5 pyramid, 6 prism, 8 hex); elNodes[nElem*8] 0-based node ids in Gambit
+ * order (entries past elNN ignored); elBc[nElem*6] boundary code of each local face
+ * (0 interior / untagged, 1 symmetry, 2 outlet, 3 inlet, 4 slip, 5 wall: the codes the reader
+ * maps 45/26/13/42/51 to).  The arrays are copied. */
+int  fg_mesh_build(int32_t nNodes, const double *nodes, int32_t nElem, const int32_t *elNN, const int32_t *elNodes,
+                   const int32_t *elBc, const fg_mesh_opts *opts, fg_mesh **out);
 int  fg_mesh_info_get(const fg_mesh *m, fg_mesh_info *info);
 int  fg_mesh_view_get(const fg_mesh *m, fg_mesh_view *view);
 /* new2old[i] = reference (.neu) index of device cell i. */
@@ -251,6 +265,12 @@ int fg_solver_set_halo(fg_solver *s, const fg_halo_ops *ops, void *sendBuf, void
  * that is not finite, has alpha outside [0, 1] or a negative partial density, and the state is
  * left as it was.  Synchronises `stream` (may be NULL). */
 int fg_set_state(fg_solver *s, const double *U, void *stream);
+/* fg_set_state without the synchronisation: the upload, the check and the replacement are
+ * queued on `stream` and the call returns at once (from pinned host memory the copy is
+ * asynchronous too: keep U unchanged until the stream has passed it).  A rejected upload leaves
+ * the state as it was and is reported by fg_check_state and by every fg_step (FG_ERR_NAN, naming
+ * the cell) until a state is uploaded successfully.  For pipelines that upload every step. */
+int fg_set_state_async(fg_solver *s, const double *U, void *stream);
 /* Download U (nElem*10 doubles, reference order).  Synchronises `stream`. */
 int fg_get_state(fg_solver *s, double *U, void *stream);
 
@@ -350,6 +370,19 @@ int fg_cons_calc(fg_solver *s, int32_t ivar, double *out, void *stream);
 #define FG_NOALLOC_MAX_CELLS (65536 * 256)
 int fg_cons_integral_noalloc(const double *U, const double *vol, int32_t nCells, int32_t ivar, double *out,
                              void *stream);
+
+/* State probe for monitoring a run (no counterpart in the reference, whose consCalc gives the
+ * integral of one variable, DP/consCalc.cu:40): vapour volume = integral of 1 - alpha (consCalc
+ * of variable 0), maximum and minimum of the mixture pressure alpha p_L + (1 - alpha) p_G and the
+ * maximum speed |u|, from the current state, by deterministic device reductions.  Synchronises
+ * `stream`.  Not available on a part of a partitioned mesh. */
+typedef struct fg_probe_out {
+    double vapourVolume;
+    double maxPressure;
+    double minPressure;
+    double maxSpeed;
+} fg_probe_out;
+int fg_probe(fg_solver *s, fg_probe_out *out, void *stream);
 
 /* dt and physical time held by the solver. */
 int fg_get_time(fg_solver *s, double *dt, double *physicalTime, int32_t *iStep);

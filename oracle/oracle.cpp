@@ -147,8 +147,10 @@ void bc_values(const fg_case *c, const double *n, const double *t1, const double
         s[4] = v[1];
         s[5] = v[2];
     } else if (bc == 3) {
-        /* Dirichlet inlet with the reference's fixed p = 11.4e5 Pa, T = 115.3 K (DP/bc.h:2-25) */
-        const double pIn = 11.4e5, tIn = 115.3;
+        /* Dirichlet inlet with the reference's fixed p = 11.4e5 Pa, T = 115.3 K (DP/bc.h:2-25), or
+         * the case's prescribed inlet state (extension) */
+        const int own = (c->inletStateFlag == 1);
+        const double pIn = own ? c->inletP : 11.4e5, tIn = own ? c->inletT : 115.3;
         s[0] = 1.0 - c->avfMin;
         s[1] = eqos(c, 0, 2, pIn, tIn);
         s[2] = eqos(c, 1, 2, pIn, tIn);

@@ -184,6 +184,9 @@ int main(int argc, char **argv) {
         if (input.consCalcFlag == 1 && iStep % input.adaptDtItr == 0) consCalc(mesh, field, sMain);
         iStep++;
     }
+    // the stage functions run on the non-blocking streams sMain / sProx: wait for all of them
+    // before the end event, so the last stage's update and relaxation are inside the timed region
+    cudaDeviceSynchronize();
     cudaEventRecord(t1, 0);
     cudaEventSynchronize(t1);
     float ms = 0;

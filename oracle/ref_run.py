@@ -18,7 +18,7 @@ EXE = HERE / "_ref" / "fooska_ref_dp"
 
 # case fields of ours that the reference's INPUT struct does not have
 EXTENSION_KEYS = ("relaxFlag", "hllcEnergyFix", "hllcTieTol", "heatFlux", "limiter", "inletVelFlag", "reserved",
-                  "inletVel")
+                  "inletVel", "inletStateFlag", "inletP", "inletT")
 
 
 def available() -> bool:

@@ -18,6 +18,12 @@ SLIP = {s: "slip" for s in ("x0", "x1", "y0", "y1", "z0", "z1")}
 # rounding noise of the precision under test.
 TIE_TOL = {"fp64": 1e-9, "mixed": 1e-4}
 
+# Factor on the mixed path's tolerances per case.  Stiffened water (p_inf = 3.43e8 Pa, 34 times
+# the 10 MPa operating pressure) forms its pressure as a difference of terms of order
+# gamma p_inf, so FP32 face states carry about 1.5 decimal digits less than with the
+# reference's fluid.
+MIXED_TOL_SCALE = {"ball_bubble": 5.0}
+
 
 def make(name: str, meshdir, prec: str = "fp64") -> tuple:
     """Return (Mesh, case, U0) for a named parity case."""
@@ -33,6 +39,8 @@ def make(name: str, meshdir, prec: str = "fp64") -> tuple:
         c.limiter = 1
         c.inletVelFlag = 1
         c.inletVel[0], c.inletVel[1], c.inletVel[2] = 30.0, 2.0, -1.0
+        c.inletStateFlag = 1
+        c.inletP, c.inletT = 9.0e5, 113.0
         ic = "perturbed"
     elif name == "tet_ref":
         if not os.path.exists(path):
@@ -60,6 +68,14 @@ def make(name: str, meshdir, prec: str = "fp64") -> tuple:
         c = cases.sod_case()
         c.adaptDtItr = 2
         ic = "sod"
+    elif name == "ball_bubble":
+        # reduced water / vapour bubble collapse: the ball generator of the 4 M-tet workload at
+        # n = 8 (3072 tets), a 2.5 mm bubble (2340 Pa) in 10 MPa water, van Albada limiter
+        path = os.path.join(str(meshdir), "ball8.neu")
+        if not os.path.exists(path):
+            meshgen.write_neu(path, meshgen.ball_tets(8))
+        c = cases.water_vapour_case()
+        ic = "bubble"
     else:
         raise KeyError(name)
     c.hllcTieTol = TIE_TOL[prec]
@@ -67,6 +83,8 @@ def make(name: str, meshdir, prec: str = "fp64") -> tuple:
     a = m.arrays()
     if ic == "perturbed":
         U = cases.perturbed_two_phase_ic(c, a["cellCenter"], seed=5, vel=25.0)
+    elif ic == "bubble":
+        U = cases.bubble_ic(c, a["cellCenter"], R0=2.5e-3, width=1e-3)
     elif ic == "tgv":
         U = cases.tgv_ic(c, a["cellCenter"])
     else:
@@ -74,4 +92,4 @@ def make(name: str, meshdir, prec: str = "fp64") -> tuple:
     return m, c, U
 
 
-NAMES = ["tet_ref", "mixed_ref_rk3", "hex_periodic_tgv", "tet_sod", "tet_ext"]
+NAMES = ["tet_ref", "mixed_ref_rk3", "hex_periodic_tgv", "tet_sod", "tet_ext", "ball_bubble"]
