@@ -225,8 +225,9 @@ def run_ours(args, rank, world, local_rank, dist):
     s.profile(False)
     mem = s.memory_bytes()
     # end to end through the C ABI with pinned host buffers: every step uploads the state
-    # (fg_set_state_async: copy, device check, scatter; no host round trip), steps, and reads the
-    # state back (fg_get_state: gather, copy, synchronise)
+    # (fg_set_state_async: copy on the solver's copy stream, device check, scatter), steps, and
+    # reads the state back (fg_get_state_async: gather, copy); the host waits once at the end, so
+    # the upload of step k+1 overlaps step k and its download
     Uin = torch.empty((nE, 10), dtype=torch.float64, pin_memory=True)
     Uin.numpy()[:] = U0
     Uout = torch.empty((nE, 10), dtype=torch.float64, pin_memory=True)
@@ -242,7 +243,7 @@ def run_ours(args, rank, world, local_rank, dist):
     for _ in range(e2e_steps):
         s.set_state_async(Uin.numpy(), stream=stream.cuda_stream)
         s.step(stream=stream.cuda_stream)
-        s.get_state(Uout.numpy(), stream=stream.cuda_stream)
+        s.get_state_async(Uout.numpy(), stream=stream.cuda_stream)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
@@ -312,7 +313,7 @@ def run_ours(args, rank, world, local_rank, dist):
         fp64_value=fp64_value, mixed_over_fp64=value / fp64_value,
         e2e={"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nE * 80, "d2h_bytes_per_step": nE * 80,
              "steps": e2e_steps, "h2d_gbs": h2d_gbs, "d2h_gbs": d2h_gbs,
-             "api": "fg_set_state_async + fg_step + fg_get_state, pinned host buffers, one stream"},
+             "api": "fg_set_state_async + fg_step + fg_get_state_async per step, pinned host buffers"},
         gpu_launches=launches,
         roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                   "traffic": traffic, "kernel": "k_face<float> + k_gather<float> (face flux, owner-side gather + RK)",
@@ -327,8 +328,14 @@ def run_ours(args, rank, world, local_rank, dist):
     if rank == 0 and not args.no_mesh_timing:
         out["mesh_preprocess"] = mesh_setup_times(path, per)
     # ---------------- two-phase bubble collapse with the Gibbs relaxation and the learned surrogate
+    sg = None
     if not args.no_two_phase:
-        out["two_phase"] = bubble(args, torch, stream, dev)
+        out["two_phase"], sg = bubble(args, torch, stream, dev)
+    # ---------------- large liquid jet (about 40 M cells)
+    if not args.no_jet:
+        out["jet"] = jet(args, torch, stream, dev, surrogate=sg)
+    if sg is not None:
+        sg.close()
     # ---------------- CPU baseline (rank 0, N = 1 only): oracle FP64 on the host cores; its final
     # state is the reference of the accuracy check of both GPU paths
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -350,11 +357,17 @@ def bubble(args, torch, stream, dev):
     Every step is timed by CUDA events; between steps (outside the timed regions) fg_probe gives
     the vapour volume and the pressure extrema.  The collapse time is the first time the vapour
     volume falls below 10 % of its initial value (linear between steps); the peak pressure is the
-    largest mixture pressure seen up to then."""
+    largest mixture pressure seen up to 20 steps after it.  The FP64 run stops there (or after
+    FG_BENCH_BALL_STEPS steps); the two mixed runs take exactly as many steps, so their final
+    states are compared with the FP64 one.
+    The limiter is the reference's (limiter = 0): with the van Albada-type extension the vapour
+    partial density of interface cells turns negative within about 60 steps at 0.1 mm spacing,
+    in the oracle as on the GPU, at any CFL number tried (0.5, 0.25); the parity tests cover that
+    limiter on a reduced ball."""
     from fooskagpu_b200 import cases, meshgen
     from fooskagpu_b200.api import Mesh, Solver, Surrogate
     n = int(os.environ.get("FG_BENCH_BALL_N", "91"))
-    steps = int(os.environ.get("FG_BENCH_BALL_STEPS", "1000"))
+    steps = int(os.environ.get("FG_BENCH_BALL_STEPS", "1600"))
     t0 = time.perf_counter()
     nm = meshgen.ball_tets(n)
     gen_s = time.perf_counter() - t0
@@ -362,7 +375,7 @@ def bubble(args, torch, stream, dev):
     mesh = Mesh.build(nm.nodes, nm.elems, nm.bcs, gpu=True, device=dev)
     pre_s = time.perf_counter() - t0
     del nm
-    case = cases.water_vapour_case()
+    case = cases.water_vapour_case(limiter=0, adapt_itr=1)
     U0 = cases.bubble_ic(case, mesh.arrays()["cellCenter"], width=1.5 * meshgen.ball_spacing(n, 1e-3))
     nE = mesh.n_elem
     res = {"workload": f"bubble_collapse_water_vapour_ball_{nE}_tets", "cells": nE, "faces": mesh.n_fcs,
@@ -371,7 +384,7 @@ def bubble(args, torch, stream, dev):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
-    def run(prec, sg=None, log=0):
+    def run(prec, nsteps, sg=None, log=0, stop_after_collapse=False):
         s = Solver(mesh, case, precision=prec, device=dev)
         s.set_state(U0)
         if log:
@@ -381,7 +394,12 @@ def bubble(args, torch, stream, dev):
         v0 = s.probe()["vapourVolume"]
         hist, ms, tc, pk, failed = [], 0.0, None, 0.0, None
         chem = fall = iters = relaxed = 0
-        for k in range(steps):
+        after = 0
+        for k in range(nsteps):
+            if stop_after_collapse and tc is not None:
+                after += 1
+                if after > 20:
+                    break
             e0.record(stream)
             try:
                 s.step(stream=stream.cuda_stream)
@@ -398,8 +416,9 @@ def bubble(args, torch, stream, dev):
             iters += st["nIter"]
             relaxed += st["nChem"] + st["nTherm"]
             t = s.time()[1]
-            if tc is None:
+            if tc is None or after <= 20:
                 pk = max(pk, pr["maxPressure"])
+            if tc is None:
                 if hist and pr["vapourVolume"] < 0.1 * v0:
                     tp, vp = hist[-1][0], hist[-1][1]
                     tc = tp + (t - tp) * (vp - 0.1 * v0) / (vp - pr["vapourVolume"])
@@ -424,7 +443,9 @@ def bubble(args, torch, stream, dev):
             out["stopped"] = r["failed"][:200]
         return out
 
-    r64 = run("fp64", log=12_000_000)
+    r64 = run("fp64", steps, log=12_000_000, stop_after_collapse=True)
+    steps = r64["steps"]
+    res["steps"] = steps
     X, Y = r64.pop("data")
     res["fp64"] = summary(r64)
     g = Surrogate(device=dev, seed=1)
@@ -436,11 +457,10 @@ def bubble(args, torch, stream, dev):
     res["surrogate_training"] = {"samples": take, "logged": int(len(X)), "epochs": epochs, "final_loss": loss,
                                  "seconds": time.perf_counter() - t0}
     del X, Y
-    rm = run("mixed")
+    rm = run("mixed", steps)
     res["mixed"] = summary(rm)
-    rs = run("mixed", sg=g)
+    rs = run("mixed", steps, sg=g)
     res["mixed_surrogate"] = summary(rs)
-    g.close()
     res["value"] = res["mixed_surrogate"]["value"]
     res["fp64_value"] = res["fp64"]["value"]
     res["mixed_surrogate_over_fp64"] = res["value"] / res["fp64_value"]
@@ -463,6 +483,81 @@ def bubble(args, torch, stream, dev):
         acc[key] = e
     acc["tolerance"] = {"rel_l2": 1e-4, "note": "rho / p relative L2 after the run against the FP64 Newton run"}
     res["accuracy_vs_fp64"] = acc
+    mesh.close()
+    return res, g
+
+
+def jet(args, torch, stream, dev, surrogate=None):
+    """Large multiphase liquid jet into pressurised gas: a cylinder of 40 D x 100 D (D = 0.2 mm)
+    meshed by meshgen.jet_cylinder (prisms in the upstream half, prisms split into tets
+    downstream; about 40 M cells at the default n = 228, 100 + 100 layers), a 200 m/s water jet
+    through a D-wide inlet into gas at 5 MPa, WALE LES, SSP-RK3 (cases.jet_case).  FP64 and mixed
+    precision, and mixed with the learned surrogate attached (the bubble run's, the same fluid);
+    each path runs the same `steps` steps after 2 warm-up steps.  Reports the device memory of
+    each solver, per-kernel times and achieved GB/s, and the mesh generation and pre-processing
+    times (the host pre-processor too with --jet-host-mesh)."""
+    from fooskagpu_b200 import cases, meshgen
+    from fooskagpu_b200.api import Mesh, Solver
+    n = int(os.environ.get("FG_BENCH_JET_N", "228"))
+    nzp = int(os.environ.get("FG_BENCH_JET_NZ", "100"))
+    steps = args.jet_steps
+    t0 = time.perf_counter()
+    nm = meshgen.jet_cylinder(n=n, nz_prism=nzp, nz_tet=nzp)
+    gen_s = time.perf_counter() - t0
+    res = {"workload": "liquid_jet_cylinder_40Dx100D_tet_prism", "steps": steps, "warmup": 2,
+           "mesh": {"generator": f"meshgen.jet_cylinder(n={n}, nz_prism={nzp}, nz_tet={nzp})", "generate_s": gen_s}}
+    t0 = time.perf_counter()
+    mesh = Mesh.build(nm.nodes, nm.elems, nm.bcs, gpu=True, device=dev)
+    res["mesh"]["gpu_preprocess_s"] = time.perf_counter() - t0
+    if args.jet_host_mesh:
+        t0 = time.perf_counter()
+        mh = Mesh.build(nm.nodes, nm.elems, nm.bcs, gpu=False)
+        res["mesh"]["host_preprocess_s"] = time.perf_counter() - t0
+        mh.close()
+    del nm
+    info = mesh.info
+    nE = mesh.n_elem
+    res.update(cells=nE, faces=info["nFcs"], tets=info["nTet"], prisms=info["nPrism"])
+    case = cases.jet_case()
+    U0 = cases.jet_ic(case, mesh.arrays()["cellCenter"])
+    nf = (4.0 * info["nTet"] + 5.0 * info["nPrism"]) / nE
+    peak, _ = _peaks()
+    for key, prec, sg in (("fp64", "fp64", None), ("mixed", "mixed", None), ("mixed_surrogate", "mixed", surrogate)):
+        if key == "mixed_surrogate" and sg is None:
+            continue
+        t0 = time.perf_counter()
+        s = Solver(mesh, case, precision=prec, device=dev)
+        create_s = time.perf_counter() - t0
+        s.set_state(U0)
+        if sg is not None:
+            s.set_surrogate(sg, 1e-6, 3)
+        for _ in range(2):
+            s.step(stream=stream.cuda_stream)
+        ms = time_steps(s, steps, torch, stream)
+        s.profile(True)
+        time_steps(s, min(steps, 5), torch, stream)
+        prof = s.profile_read()
+        s.profile(False)
+        st = s.relax_stats()
+        s.check_state()
+        bg, bf = algorithmic_bytes(nf, fp64=(prec == "fp64"))
+        k = {kk: v["ms"] / v["launches"] for kk, v in prof.items()}
+        gbs = {}
+        if "grad" in k:
+            gbs["grad"] = bg * nE / (k["grad"] / 1e3) / 1e9
+        if "flux" in k and "gather" in k:
+            gbs["face+gather"] = bf * nE / ((k["flux"] + k["gather"]) / 1e3) / 1e9
+        res[key] = {"value": nE * case.rkSteps * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                    "device_memory_gb": s.memory_bytes() / 1e9, "solver_create_s": create_s,
+                    "kernels_ms": k, "achieved_gbs": gbs,
+                    "hbm_frac": {kk: v / peak for kk, v in gbs.items()},
+                    "relaxation": {"chem_cells": st["nChem"], "fallback": st["nFallback"]}}
+        s.close()
+    res["value"] = res.get("mixed_surrogate", res["mixed"])["value"]
+    res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    res["value_over_fp64"] = res["value"] / res["fp64"]["value"]
+    res["bytes_model"] = f"per cell-stage: pass G {algorithmic_bytes(nf, False)[0]:.0f} B, pass F " \
+                         f"{algorithmic_bytes(nf, False)[1]:.0f} B (mixed; faces per cell {nf:.2f})"
     mesh.close()
     return res
 
@@ -573,6 +668,74 @@ def reference_gpu(args):
             "build": "reference DP sources, nvcc 12.9 -gencode sm_100a -rdc, -maxrregcount=128, single-rank MPI/METIS stubs"}
 
 
+def run_partitioned(args, rank, world, local_rank, dist):
+    """--partition: the TGV mesh split into `world` parts (space-filling-curve ranges of the
+    device order, fg_mesh_partition), one part per GPU, the halo records of every RK stage moved
+    by fooskagpu_b200.halo.TorchHalo over NCCL (device buffers, point to point), dt and the
+    conservation integral combined with all-reduce.  The whole job's work is fixed (strong
+    scaling); value = all cells x RK stages x steps / the slowest rank's time."""
+    import torch
+    from fooskagpu_b200 import cases
+    from fooskagpu_b200.api import Mesh, Solver
+    from fooskagpu_b200.halo import TorchHalo
+    torch.cuda.set_device(local_rank)
+    dev = local_rank
+    path, per = tgv_mesh(rank, world, dist)
+    mesh = Mesh.load_neu(path, scale=1.0, periodic=per, gpu=True, device=dev)
+    nE = mesh.n_elem
+    case = bench_tgv_case()
+    U0 = cases.tgv_ic(case, mesh.arrays()["cellCenter"])
+    part = mesh.partition(world, rank)
+    cg = part.partition_maps()["cell_global"][:part.n_owned]
+    stream = torch.cuda.Stream(device=dev)
+    s = Solver(part, case, precision="mixed", device=dev)
+    halo = TorchHalo(s, part, device=f"cuda:{dev}")
+    Up = np.ascontiguousarray(U0[cg])
+    s.set_state(Up)
+    for _ in range(args.warmup):
+        s.step(stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = Clocks(dev)
+    clocks.start()
+    n0 = s.launch_count()
+    ms = rank_max(time_steps(s, args.steps, torch, stream), dist, f"cuda:{dev}")
+    cl = clocks.stop()
+    launches = s.launch_count() - n0
+    value = nE * case.rkSteps * args.steps / (ms / 1e3)
+    # end to end: each rank uploads its part, steps and reads it back
+    Uin = torch.empty(Up.shape, dtype=torch.float64, pin_memory=True)
+    Uin.numpy()[:] = Up
+    Uout = torch.empty(Up.shape, dtype=torch.float64, pin_memory=True)
+    e2e_steps = max(3, min(args.steps, 20))
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        s.set_state_async(Uin.numpy(), stream=stream.cuda_stream)
+        s.step(stream=stream.cuda_stream)
+        s.get_state(Uout.numpy(), stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = rank_max(e0.elapsed_time(e1), dist, f"cuda:{dev}")
+    info = part.part_info
+    halo_cells = torch.tensor([info["nGhost"]], dtype=torch.float64, device=f"cuda:{dev}")
+    dist.all_reduce(halo_cells)
+    s.close()
+    return dict(
+        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+        ms_per_step=ms / args.steps, higher_is_better=True, scaling="strong", vs_baseline=None,
+        dtype="fp32 face math + fp64 state/RK (mixed)", data="synthetic",
+        config={"workload": f"tgv_les_wale_{NCELL_SIDE}^3_hex_periodic", "cells": nE, "rk_stages": case.rkSteps,
+                "parallelism": f"partitioned mesh, {world} parts (space-filling-curve ranges), NCCL halo per stage",
+                "ghost_cells_total": int(halo_cells.item()), "halo_exchanges_per_step": 2 * case.rkSteps},
+        e2e={"value": nE * case.rkSteps * e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+             "h2d_bytes_per_step": nE * 80, "d2h_bytes_per_step": nE * 80, "steps": e2e_steps},
+        gpu_launches=launches, clocks=cl)
+
+
 def run_reference(args):
     """Reference arm.  The reference implements this path only in CUDA, so its CPU arm is the FP64
     C++ restatement of it (oracle), on all host threads, on the same workload: the same mesh
@@ -628,6 +791,11 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true", help="reference arm: skip timing the reference GPU build")
     ap.add_argument("--no-two-phase", action="store_true", help="skip the two-phase (surrogate) workload")
     ap.add_argument("--no-mesh-timing", action="store_true", help="skip timing the host vs GPU mesh pre-processor")
+    ap.add_argument("--no-jet", action="store_true", help="skip the 40 M-cell liquid jet")
+    ap.add_argument("--partition", action="store_true",
+                    help="N > 1: one partitioned mesh over the N GPUs (NCCL halo) instead of N replicas")
+    ap.add_argument("--jet-steps", type=int, default=20, help="timed steps per path of the jet (the configuration: 200)")
+    ap.add_argument("--jet-host-mesh", action="store_true", help="also time the host pre-processor on the jet mesh")
     ap.add_argument("--n", type=int, default=None, help="cells per side of the TGV cube (default 128)")
     args = ap.parse_args()
     if args.n:
@@ -652,7 +820,10 @@ def main():
         D.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device(f"cuda:{local_rank}"))
         dist = D
     try:
-        out = run_ours(args, rank, world, local_rank, dist)
+        if args.partition and dist is not None:
+            out = run_partitioned(args, rank, world, local_rank, dist)
+        else:
+            out = run_ours(args, rank, world, local_rank, dist)
         if rank == 0:
             print(json.dumps(out), flush=True)
     finally:

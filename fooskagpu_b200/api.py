@@ -180,6 +180,12 @@ class Solver:
             raise ValueError("set_state_async needs a C-contiguous float64 array of shape (n, 10)")
         check(lib().fg_set_state_async(self._h, _dptr(U), stream))
 
+    def get_state_async(self, out: np.ndarray, stream: Optional[int] = None) -> None:
+        """Queue the download into `out` (fg_get_state_async); complete once the stream has passed it."""
+        if not (out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.shape == (self.n, 10)):
+            raise ValueError("get_state_async needs a C-contiguous float64 array of shape (n, 10)")
+        check(lib().fg_get_state_async(self._h, _dptr(out), stream))
+
     def get_state(self, out: Optional[np.ndarray] = None, stream: Optional[int] = None) -> np.ndarray:
         if out is None:
             out = np.empty((self.n, 10), dtype=np.float64)

@@ -228,22 +228,26 @@ def water_vapour_case(rk=3, cfl=0.5, adapt_itr=10, limiter=1, viscous=True, base
 
 
 def bubble_ic(case: FgCase, centres: np.ndarray, R0=1e-3, p_bubble=2340.0, p_liquid=1e7, T=298.15,
-              width=1e-4) -> np.ndarray:
+              width=1e-4, u_wall=0.0) -> np.ndarray:
     """Rayleigh bubble: vapour (liquid volume fraction avfMin) inside radius R0 at p_bubble, liquid
     (1 - avfMin) outside with the Rayleigh-Plesset pressure field p = p_liquid + (p_bubble -
-    p_liquid) R0 / r (continuous at R0, p_liquid far away), at rest, uniform temperature T; the
-    volume fraction changes over a tanh profile of the given width.  At T = 298.15 K the
-    saturation pressure of the model is above p_bubble, so the liquid of the interface cells is
-    superheated and the Gibbs relaxation acts there."""
+    p_liquid) R0 / r (continuous at R0, p_liquid far away), uniform temperature T; the volume
+    fraction changes over a tanh profile of the given width.  At rest by default; u_wall != 0
+    gives the radial flow of a bubble wall moving at u_wall, u = u_wall (R0 / r)^2 outside and
+    u_wall r / R0 inside.  At T = 298.15 K the saturation pressure of the model is above
+    p_bubble, so the liquid of the interface cells is superheated and the Gibbs relaxation acts
+    there."""
     r = np.linalg.norm(centres, axis=1)
     amin = case.avfMin
     alpha = amin + (1 - 2 * amin) * 0.5 * (1 + np.tanh((r - R0) / width))
     p = np.where(r <= R0, p_bubble, p_liquid + (p_bubble - p_liquid) * R0 / np.maximum(r, 1e-30))
     rl = rho_of_pT(case, 0, p, T)
     rg = rho_of_pT(case, 1, p, T)
-    z = np.zeros_like(r)
+    ur = np.where(r <= R0, u_wall * r / R0, u_wall * (R0 / np.maximum(r, 1e-30)) ** 2)
+    rhat = centres / np.maximum(r, 1e-30)[:, None]
+    vel = ur[:, None] * rhat
     mv = (1 - alpha) * rg
-    return prim_to_cons(case, alpha, rl, rg, z, z, z, p, p, mv)
+    return prim_to_cons(case, alpha, rl, rg, vel[:, 0], vel[:, 1], vel[:, 2], p, p, mv)
 
 
 def mixture_pressure(case: FgCase, U: np.ndarray) -> np.ndarray:
@@ -258,3 +262,30 @@ def mixture_pressure(case: FgCase, U: np.ndarray) -> np.ndarray:
         pm = (g - 1) * rho * e - g * case.pInf[m] - (g - 1) * case.eta[m] * rho
         out += vol * pm
     return out
+
+
+# ---------------------------------------------------------------- liquid jet into pressurised gas
+def jet_case(u_jet=200.0, p_gas=5e6, T=298.15, rk=3, cfl=0.3, base=None) -> FgCase:
+    """Water jet at u_jet through the inlet (bc 3) into gas at p_gas: the water / vapour constants
+    of water_vapour_case with the WALE eddy viscosity (turbulence = 1; Re_D = rho u D / mu = 4e4
+    for D = 0.2 mm), the reference's limiter, and the inlet extensions: prescribed inlet velocity
+    (0, 0, u_jet) and the inlet state (p_gas, T) instead of the reference's fixed one.  The time
+    step adapts every step at CFL 0.3: the CFL bound sees the gas until the liquid (four times
+    the sound speed) has entered a cell, and a dt held over ten steps blows up at the inlet."""
+    c = water_vapour_case(rk=rk, cfl=cfl, adapt_itr=1, limiter=0, viscous=True, base=base)
+    c.turbulence = 1
+    c.inletVelFlag = 1
+    c.inletVel[0], c.inletVel[1], c.inletVel[2] = 0.0, 0.0, u_jet
+    c.inletStateFlag = 1
+    c.inletP, c.inletT = p_gas, T
+    return c
+
+
+def jet_ic(case: FgCase, centres: np.ndarray, p_gas=5e6, T=298.15) -> np.ndarray:
+    """Gas (liquid volume fraction avfMin) at p_gas and T, at rest, everywhere."""
+    n = len(centres)
+    p = np.full(n, p_gas)
+    rl = rho_of_pT(case, 0, p, T)
+    rg = rho_of_pT(case, 1, p, T)
+    z = np.zeros(n)
+    return prim_to_cons(case, np.full(n, case.avfMin), rl, rg, z, z, z, p, p, (1 - case.avfMin) * rg)

@@ -158,14 +158,16 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
         constexpr int TPV = vpv<T>();
         constexpr int WV = (NP + TPV - 1) / TPV;   // vectors holding the NP used values
         const V *Wv = reinterpret_cast<const V *>(W);
-        for (int i = threadIdx.x; i < nRec * WV; i += blockDim.x) {
-            const int q = i / nRec, r = i - q * nRec;
+        for (int r = threadIdx.x; r < nRec; r += blockDim.x) {
             const int src = staged_source(m, b, r, lo, nBlockRecs);
             if (src < 0) continue;
-            const V x = __ldg(Wv + (size_t)q * m.n + src);
 #pragma unroll
-            for (int j = 0; j < TPV; j++)
-                if (q * TPV + j < NP) rec[r * WS + q * TPV + j] = vlane(x, j);
+            for (int q = 0; q < WV; q++) {
+                const V x = __ldg(Wv + (size_t)q * m.n + src);
+#pragma unroll
+                for (int j = 0; j < TPV; j++)
+                    if (q * TPV + j < NP) rec[r * WS + q * TPV + j] = vlane(x, j);
+            }
         }
     }
     stage_geometry(m, lo, nOwn, sg, sl);

@@ -81,7 +81,18 @@ constexpr int FREC = 12;
 template <typename T> struct MinBlocks {
     static constexpr int grad = FG_GRAD_MINB, face = FG_FACE_MINB, gather = FG_GATHER_MINB;
 };
-template <> struct MinBlocks<double> { static constexpr int grad = 0, face = 0, gather = 0; };
+#ifndef FG_GRAD_MINB_D
+#define FG_GRAD_MINB_D 0
+#endif
+#ifndef FG_FACE_MINB_D
+#define FG_FACE_MINB_D 0
+#endif
+#ifndef FG_GATHER_MINB_D
+#define FG_GATHER_MINB_D 0
+#endif
+template <> struct MinBlocks<double> {
+    static constexpr int grad = FG_GRAD_MINB_D, face = FG_FACE_MINB_D, gather = FG_GATHER_MINB_D;
+};
 template <typename T> struct StageCells { static constexpr int value = FG_STAGE_CELLS_F; };
 template <> struct StageCells<double> { static constexpr int value = FG_STAGE_CELLS_D; };
 

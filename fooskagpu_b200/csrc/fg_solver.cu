@@ -71,7 +71,15 @@ struct fg_solver {
     virtual ~fg_solver() {
         for (cudaEvent_t e : evPool) cudaEventDestroy(e);
         if (hBad) cudaFreeHost((void *)hBad);
+        if (evInFree) cudaEventDestroy(evInFree);
+        if (evCopied) cudaEventDestroy(evCopied);
+        if (copyStream) cudaStreamDestroy(copyStream);
     }
+    // asynchronous uploads copy on their own stream into their own staging buffer, so the copy of
+    // the next state overlaps the work queued before it (created on the first asynchronous upload)
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t evInFree = nullptr;   // the last scatter has read the upload staging buffer
+    cudaEvent_t evCopied = nullptr;   // the upload copy has landed
     int init_flag() {
         void *h = nullptr;
         FG_CUDA_TRY(cudaHostAlloc(&h, 2 * sizeof(int32_t), cudaHostAllocMapped));
@@ -181,7 +189,8 @@ struct fg_solver {
     // upload U; wait = true synchronises and reports a rejected upload, false leaves the report to
     // the flags (fg_step / fg_check_state)
     virtual int set_state(const double *U, cudaStream_t s, bool wait) = 0;
-    virtual int get_state(double *U, cudaStream_t s) = 0;
+    // download U; wait = false leaves the copy queued on the stream
+    virtual int get_state(double *U, cudaStream_t s, bool wait) = 0;
     virtual int compute_rhs(int wantSignal, cudaStream_t s) = 0;
     virtual int time_step(double *dtOut, cudaStream_t s) = 0;
     virtual int init_rk(cudaStream_t s) = 0;
@@ -248,6 +257,7 @@ template <typename T>
 struct SolverT : public fg_solver {
     DevBuf dNbr, dFlags, dGeo, dVol, dVolP, dNew2Old, dHaloStart, dHaloIds, dSlotLocal;
     DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dBlockMin, dScal, dCnt, dCons, dStage;
+    DevBuf dStageIn;   // staging buffer of the asynchronous uploads (on first use)
     DevBuf dFIdx, dFGeo, dSlotFace, dClosure, dFB;
     DevBuf dOrdFlag, dOrdCnt, dOrdOff, dOrder, dOrdTotal;   // relaxation cell ordering
     DevBuf dPred, dHullOk, dTcErr;                          // surrogate predictions
@@ -608,16 +618,36 @@ struct SolverT : public fg_solver {
     }
 
     int set_state(const double *U, cudaStream_t s, bool wait) override {
-        FG_CUDA_TRY(cudaMemcpyAsync(dStage.p, U, (size_t)nU * NV * sizeof(double), cudaMemcpyHostToDevice, s));
+        const size_t ub = (size_t)nU * NV * sizeof(double);
+        double *stage = dStage.as<double>();
+        if (wait) {
+            FG_CUDA_TRY(cudaMemcpyAsync(dStage.p, U, ub, cudaMemcpyHostToDevice, s));
+        } else {
+            if (!copyStream) {
+                FG_CUDA_TRY(dStageIn.alloc(ub));
+                bytes += dStageIn.bytes;
+                FG_CUDA_TRY(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
+                FG_CUDA_TRY(cudaEventCreateWithFlags(&evInFree, cudaEventDisableTiming));
+                FG_CUDA_TRY(cudaEventCreateWithFlags(&evCopied, cudaEventDisableTiming));
+                FG_CUDA_TRY(cudaEventRecord(evInFree, s));
+            }
+            // the copy waits only until the previous asynchronous upload has been scattered; the
+            // check and the scatter wait for the copy and follow the work queued on `s`
+            FG_CUDA_TRY(cudaStreamWaitEvent(copyStream, evInFree, 0));
+            FG_CUDA_TRY(cudaMemcpyAsync(dStageIn.p, U, ub, cudaMemcpyHostToDevice, copyStream));
+            FG_CUDA_TRY(cudaEventRecord(evCopied, copyStream));
+            FG_CUDA_TRY(cudaStreamWaitEvent(s, evCopied, 0));
+            stage = dStageIn.as<double>();
+        }
         // checked on the device; the scatter replaces the state only if every cell is usable
         prof_begin(FG_K_OTHER, s);
-        launch_check_state(nU, dStage.as<double>(), dChk.as<int32_t>(), s);
+        launch_check_state(nU, stage, dChk.as<int32_t>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("set_state check");
         prof_begin(FG_K_OTHER, s);
-        launch_scatter_state(nU, dStage.as<double>(), dNew2Old.as<int32_t>(), dU.as<double>(), dChk.as<int32_t>(),
-                             dBad, s);
+        launch_scatter_state(nU, stage, dNew2Old.as<int32_t>(), dU.as<double>(), dChk.as<int32_t>(), dBad, s);
         prof_end(s);
+        if (!wait) FG_CUDA_TRY(cudaEventRecord(evInFree, s));
         prof_begin(FG_K_OTHER, s);
         launch_prim<T>(nU, dU.as<double>(), dW[cur].as<T>(), (size_t)n, D, s);
         prof_end(s);
@@ -631,13 +661,13 @@ struct SolverT : public fg_solver {
         }
         return FG_OK;
     }
-    int get_state(double *U, cudaStream_t s) override {
+    int get_state(double *U, cudaStream_t s, bool wait) override {
         prof_begin(FG_K_OTHER, s);
         launch_gather_state(nU, dU.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("get_state");
         FG_CUDA_TRY(cudaMemcpyAsync(U, dStage.p, (size_t)nU * NV * sizeof(double), cudaMemcpyDeviceToHost, s));
-        FG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (wait) FG_CUDA_TRY(cudaStreamSynchronize(s));
         return FG_OK;
     }
     StageCoef coef(int irk, int writeU0) const {
@@ -1146,7 +1176,12 @@ int fg_set_state_async(fg_solver *s, const double *U, void *stream) {
 int fg_get_state(fg_solver *s, double *U, void *stream) {
     FG_ENTER(s);
     if (!U) return set_err(FG_ERR_ARG, "fg_get_state: null U");
-    return s->get_state(U, (cudaStream_t)stream);
+    return s->get_state(U, (cudaStream_t)stream, true);
+}
+int fg_get_state_async(fg_solver *s, double *U, void *stream) {
+    FG_ENTER(s);
+    if (!U) return set_err(FG_ERR_ARG, "fg_get_state_async: null U");
+    return s->get_state(U, (cudaStream_t)stream, false);
 }
 int fg_compute_rhs(fg_solver *s, int32_t want_signal, void *stream) {
     FG_ENTER(s);
@@ -1272,7 +1307,7 @@ int fg_checkpoint_write(fg_solver *s, const char *path) {
     FG_ENTER(s);
     if (!path) return set_err(FG_ERR_ARG, "fg_checkpoint_write: null path");
     std::vector<double> U((size_t)s->nU * fg::NV);
-    int rc = s->get_state(U.data(), 0);
+    int rc = s->get_state(U.data(), 0, true);
     if (rc != FG_OK) return rc;
     CkHeader h{};
     std::memcpy(h.magic, kCkMagic, 8);

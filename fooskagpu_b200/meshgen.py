@@ -299,41 +299,52 @@ def _split_prisms(pts, pr):
     return el
 
 
-def jet_cylinder(n: int = 224, nz_prism: int = 100, nz_tet: int = 100, diameter: float = 0.2e-3,
+def jet_cylinder(n: int = 228, nz_prism: int = 100, nz_tet: int = 100, diameter: float = 0.2e-3,
                  radius_d: float = 20.0, length_d: float = 100.0, beta: float = 3.0, jitter: float = 0.1,
                  seed: int = 20261203) -> NeuMesh:
     """Cylinder of radius radius_d * D and length length_d * D along z, meshed by extrusion: a
-    disk of 2 n^2 triangles (an n x n lattice of [-1, 1]^2 mapped onto the disk as ball_tets maps
-    the cube, graded toward the axis with sinh(beta rho) / sinh(beta), interior points jittered by
-    U(-jitter, jitter) lattice spacings, seeded), extruded through nz_prism + nz_tet layers of
-    equal thickness (interior layer heights jittered the same way).  The first nz_prism layers
-    are prisms, the rest prisms split into 3 tets each (_split_prisms): 2 n^2 (nz_prism +
-    3 nz_tet) cells.  Boundaries: the z = 0 disk is an inlet inside radius D / 2 and a wall
-    outside it; z = length is an outlet; the side is a slip wall."""
+    disk of triangles (an n x n lattice of [-1, 1]^2 stretched per axis toward the axis,
+    x = R sinh(beta xi) / sinh(beta), interior points jittered by U(-jitter, jitter) lattice
+    spacings (seeded); the lattice squares whose centre lies inside radius R are kept, a stepped
+    rim, and split into 2 triangles each), extruded through nz_prism + nz_tet layers of equal
+    thickness (interior layer heights jittered the same way).  The first nz_prism layers are
+    prisms, the rest prisms split into 3 tets each (_split_prisms).  Boundaries: the z = 0 disk is
+    an inlet inside radius D / 2 and a wall outside it; z = length is an outlet; the side is a
+    slip wall.  (A lattice mapped onto the round disk would flatten the cells at the images of the
+    square's corners.)"""
     R = radius_d * diameter
     Lz = length_d * diameter
     rng = np.random.default_rng(seed)
     i, j = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
     i, j = i.ravel(), j.ravel()
     xi = np.stack([i, j], axis=1) * (2.0 / n) - 1.0
-    rim = (i == 0) | (i == n) | (j == 0) | (j == n)
-    xi = xi + rng.uniform(-jitter, jitter, size=xi.shape) * (2.0 / n) * (~rim)[:, None]
-    rho = np.abs(xi).max(axis=1)
-    r2 = np.linalg.norm(xi, axis=1)
-    d = np.zeros_like(xi)
-    ok = rho > 0
-    sq = (rho * rho)[ok, None]
-    d[ok] = (1 - sq) * xi[ok] / rho[ok, None] + sq * xi[ok] / r2[ok, None]
-    xy = R * (np.sinh(beta * rho) / np.sinh(beta))[:, None] * d
+    edge = (i == 0) | (i == n) | (j == 0) | (j == n)
+    xi = xi + rng.uniform(-jitter, jitter, size=xi.shape) * (2.0 / n) * (~edge)[:, None]
+    xy_all = R * np.sinh(beta * xi) / np.sinh(beta)
     nid2 = lambda a, b: a * (n + 1) + b
     a0, b0 = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
     a0, b0 = a0.ravel(), b0.ravel()
     q00, q10, q01, q11 = nid2(a0, b0), nid2(a0 + 1, b0), nid2(a0, b0 + 1), nid2(a0 + 1, b0 + 1)
+    keep = np.linalg.norm(0.25 * (xy_all[q00] + xy_all[q10] + xy_all[q01] + xy_all[q11]), axis=1) < R
+    q00, q10, q01, q11 = q00[keep], q10[keep], q01[keep], q11[keep]
     tri = np.concatenate([np.stack([q00, q10, q11], axis=1), np.stack([q00, q11, q01], axis=1)])
+    used = np.unique(tri)
+    remap = np.full(len(xy_all), -1, dtype=np.int64)
+    remap[used] = np.arange(len(used))
+    tri = remap[tri]
+    xy = xy_all[used]
     # counter-clockwise in (x, y), so a prism extruded along +z has positive volume
     e1, e2 = xy[tri[:, 1]] - xy[tri[:, 0]], xy[tri[:, 2]] - xy[tri[:, 0]]
     cw = e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0] < 0
     tri[cw] = tri[cw][:, [0, 2, 1]]
+    # rim: the edges that belong to one triangle only
+    ed = np.sort(np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]]), axis=1)
+    ek = ed[:, 0] * len(xy) + ed[:, 1]
+    uk, cnt = np.unique(ek, return_counts=True)
+    rim_keys = uk[cnt == 1]
+    rim = np.zeros(len(xy), dtype=bool)
+    rim[rim_keys // len(xy)] = True
+    rim[rim_keys % len(xy)] = True
     nz = nz_prism + nz_tet
     z = np.linspace(0.0, Lz, nz + 1)
     z[1:-1] += rng.uniform(-jitter, jitter, size=nz - 1) * (Lz / nz)
@@ -349,27 +360,33 @@ def jet_cylinder(n: int = 224, nz_prism: int = 100, nz_tet: int = 100, diameter:
     prisms = pr[:nz_prism * ntri]
     tets = _split_prisms(nodes, pr[nz_prism * ntri:])
     blocks = [prisms, tets]
-    # boundary faces: all nodes on z = 0 / z = Lz / the rim
-    on_rim = np.tile(rim, nz + 1)
+    # boundary faces, searched only among the elements that can have one: the first and last
+    # layer and the columns over disk triangles with a rim edge
     kz = np.repeat(np.arange(nz + 1), n2)
+    rim_tri = np.nonzero(rim[tri].sum(axis=1) >= 2)[0]
+    lay_t = np.arange(nz_tet)
+    cand = [np.unique(np.concatenate([np.arange(ntri), (np.arange(nz_prism)[:, None] * ntri + rim_tri).ravel()]))
+            if nz_prism else np.zeros(0, dtype=np.int64),
+            np.unique(np.concatenate([(((nz_tet - 1) * ntri + np.arange(ntri))[:, None] * 3 + np.arange(3)).ravel(),
+                                      ((lay_t[:, None] * ntri + rim_tri)[:, :, None] * 3 + np.arange(3)).ravel()]))
+            if nz_tet else np.zeros(0, dtype=np.int64)]
     bcs = {}
     off = 0
-    for blk in blocks:
+    for blk, cnd in zip(blocks, cand):
         nn = blk.shape[1]
         for fi, fnodes in enumerate(FACES[nn]):
-            fn = blk[:, list(fnodes)]
+            fn = blk[cnd][:, list(fnodes)]
             bottom = np.all(kz[fn] == 0, axis=1)
             top = np.all(kz[fn] == nz, axis=1)
-            # a side face spans one rim edge: its nodes project onto two adjacent rim points
+            # a side face spans one rim edge: its nodes project onto the two ends of a rim edge
             f2 = fn % n2
             lo2, hi2 = f2.min(axis=1), f2.max(axis=1)
             two = np.all((f2 == lo2[:, None]) | (f2 == hi2[:, None]), axis=1) & (lo2 != hi2)
-            adj = (np.abs(i[lo2] - i[hi2]) + np.abs(j[lo2] - j[hi2])) == 1
-            side = np.all(on_rim[fn], axis=1) & two & adj
-            rc = np.linalg.norm(nodes[fn][:, :, :2].mean(axis=1), axis=1)
+            side = two & np.isin(lo2 * n2 + hi2, rim_keys)
+            rc = np.linalg.norm(xy[f2].mean(axis=1), axis=1)
             for name, sel in (("inlet", bottom & (rc < 0.5 * diameter)), ("wall", bottom & (rc >= 0.5 * diameter)),
                               ("outlet", top), ("slip", side & ~bottom & ~top)):
-                el = np.nonzero(sel)[0]
+                el = cnd[np.nonzero(sel)[0]]
                 if not len(el):
                     continue
                 code = BC_CODES[name]

@@ -265,14 +265,19 @@ int fg_solver_set_halo(fg_solver *s, const fg_halo_ops *ops, void *sendBuf, void
  * that is not finite, has alpha outside [0, 1] or a negative partial density, and the state is
  * left as it was.  Synchronises `stream` (may be NULL). */
 int fg_set_state(fg_solver *s, const double *U, void *stream);
-/* fg_set_state without the synchronisation: the upload, the check and the replacement are
- * queued on `stream` and the call returns at once (from pinned host memory the copy is
- * asynchronous too: keep U unchanged until the stream has passed it).  A rejected upload leaves
- * the state as it was and is reported by fg_check_state and by every fg_step (FG_ERR_NAN, naming
- * the cell) until a state is uploaded successfully.  For pipelines that upload every step. */
+/* fg_set_state without the synchronisation, for pipelines that upload every step: the call
+ * returns at once.  The copy runs on the solver's own copy stream into its own staging buffer
+ * (so it overlaps the work already queued on `stream`, such as the previous step and its
+ * download); the check and the replacement are queued on `stream` after it.  From pinned host
+ * memory the copy is asynchronous: keep U unchanged until `stream` has passed the replacement.
+ * A rejected upload leaves the state as it was and is reported by fg_check_state and by every
+ * fg_step (FG_ERR_NAN, naming the cell) until a state is uploaded successfully. */
 int fg_set_state_async(fg_solver *s, const double *U, void *stream);
 /* Download U (nElem*10 doubles, reference order).  Synchronises `stream`. */
 int fg_get_state(fg_solver *s, double *U, void *stream);
+/* fg_get_state queued on `stream` without the synchronisation: U (pinned host memory for an
+ * asynchronous copy) is complete once `stream` has passed the call. */
+int fg_get_state_async(fg_solver *s, double *U, void *stream);
 
 /* ---------------------------------------------------------------- stage functions */
 

@@ -10,9 +10,15 @@
   (oracle/_ref/fooska_ref_dp) on a B200, see ``run_stage_fixtures`` (run on a machine with the
   GPU into <outdir>, then packed here by ``collect``).
 
+* ``long_tgv16_slip.npz`` — the reference CUDA binary's state after 10, 30 and 60 full steps of a
+  16^3 slip-wall Taylor-Green vortex (``long_spec``), for the long-run comparison of the oracle and
+  the device path.
+
 usage: python tests/golden/make_golden.py kat
        python tests/golden/make_golden.py stage <outdir>     (GPU box)
        python tests/golden/make_golden.py collect <outdir>   (pack the GPU run into stage_*.npz)
+       python tests/golden/make_golden.py long <outdir>      (GPU box)
+       python tests/golden/make_golden.py collect_long <outdir>
 """
 from __future__ import annotations
 
@@ -259,6 +265,45 @@ def collect_stage_fixtures(outdir):
         print("wrote", HERE / f"stage_{spec['name']}.npz")
 
 
+# ------------------------------------------------------------------ long-run fixture (reference CUDA binary)
+LONG_STEPS = (10, 30, 60)
+
+
+def long_spec():
+    """16^3 Taylor-Green vortex in a 2 pi cube with slip walls (the reference has no periodic
+    boundary; u . n vanishes on the cube faces), the single-phase ideal gas at Mach 0.1,
+    Re 1600, WALE, SSP-RK3, the reference's dt every 100 steps and relaxation every step."""
+    L = 2 * np.pi
+    m = meshgen.box_hexes(16, 16, 16, L=(L, L, L), seed=SEED)
+    c = cases.tgv_case(pr=0.0)
+    return m, c
+
+
+def run_long_fixture(outdir):
+    from oracle import ref_run
+    outdir = Path(outdir).resolve()
+    m, c = long_spec()
+    U = cases.tgv_ic(c, centres_of(m))
+    for k in LONG_STEPS:
+        wd = outdir / f"long{k}"
+        wd.mkdir(parents=True, exist_ok=True)
+        meshgen.write_neu(str(wd / "sh.neu"), m)
+        print(k, ref_run.run(wd, wd / "sh.neu", c, U, k))
+
+
+def collect_long_fixture(outdir):
+    outdir = Path(outdir)
+    m, c = long_spec()
+    U = cases.tgv_ic(c, centres_of(m))
+    d = {"ic": U, "steps": np.array(LONG_STEPS)}
+    for k in LONG_STEPS:
+        wd = outdir / f"long{k}"
+        d[f"U{k}"] = np.fromfile(wd / "ref_U.bin", dtype=np.float64).reshape(m.n_elem, 10)
+        d[f"time{k}"] = np.array(float((wd / "ref_time.txt").read_text().split()[3]))
+    np.savez_compressed(HERE / "long_tgv16_slip.npz", **d)
+    print("wrote", HERE / "long_tgv16_slip.npz")
+
+
 if __name__ == "__main__":
     cmd = sys.argv[1] if len(sys.argv) > 1 else "kat"
     if cmd == "kat":
@@ -267,3 +312,7 @@ if __name__ == "__main__":
         run_stage_fixtures(sys.argv[2])
     elif cmd == "collect":
         collect_stage_fixtures(sys.argv[2])
+    elif cmd == "long":
+        run_long_fixture(sys.argv[2])
+    elif cmd == "collect_long":
+        collect_long_fixture(sys.argv[2])

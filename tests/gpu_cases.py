@@ -18,11 +18,24 @@ SLIP = {s: "slip" for s in ("x0", "x1", "y0", "y1", "z0", "z1")}
 # rounding noise of the precision under test.
 TIE_TOL = {"fp64": 1e-9, "mixed": 1e-4}
 
-# Factor on the mixed path's tolerances per case.  Stiffened water (p_inf = 3.43e8 Pa, 34 times
-# the 10 MPa operating pressure) forms its pressure as a difference of terms of order
-# gamma p_inf, so FP32 face states carry about 1.5 decimal digits less than with the
-# reference's fluid.
-MIXED_TOL_SCALE = {"ball_bubble": 5.0}
+# Tolerances that differ per case.  Stiffened water (p_inf = 3.43e8 Pa, 34 times the 10 MPa
+# operating pressure) forms its pressure as a difference of terms of order gamma p_inf:
+#  - FP32 face states leave about 1.3 decimal digits less than with the reference's fluid in a
+#    single residual evaluation (mixed path, factor 20 on its residual / gradient tolerances);
+#  - the collapsing bubble amplifies any perturbation of the state: in the FP64 oracle itself a
+#    relative perturbation of 1e-15 of the initial state changes the state after 3 steps by
+#    2e-7 relative, so round-off differences between two correct implementations (FMA
+#    contraction, summation order) show up at that level after a few steps.
+CASE_TOL = {"ball_bubble": {"fp64": {"state": 2e-6},
+                            "mixed": {"rhs": 4e-3, "grad": 6e-3, "theta": 6e-3, "signal": 4e-5, "dt": 4e-5,
+                                      "state": 1e-3}}}
+
+
+def case_tol(name: str, prec: str, base: dict) -> dict:
+    """`base` (tolerances by key) with the case's overrides."""
+    out = dict(base)
+    out.update(CASE_TOL.get(name, {}).get(prec, {}))
+    return out
 
 
 def make(name: str, meshdir, prec: str = "fp64") -> tuple:
@@ -70,7 +83,7 @@ def make(name: str, meshdir, prec: str = "fp64") -> tuple:
         ic = "sod"
     elif name == "ball_bubble":
         # reduced water / vapour bubble collapse: the ball generator of the 4 M-tet workload at
-        # n = 8 (3072 tets), a 2.5 mm bubble (2340 Pa) in 10 MPa water, van Albada limiter
+        # n = 8, a 2.5 mm bubble (2340 Pa) in 10 MPa water collapsing at 20 m/s, van Albada limiter
         path = os.path.join(str(meshdir), "ball8.neu")
         if not os.path.exists(path):
             meshgen.write_neu(path, meshgen.ball_tets(8))
@@ -84,7 +97,7 @@ def make(name: str, meshdir, prec: str = "fp64") -> tuple:
     if ic == "perturbed":
         U = cases.perturbed_two_phase_ic(c, a["cellCenter"], seed=5, vel=25.0)
     elif ic == "bubble":
-        U = cases.bubble_ic(c, a["cellCenter"], R0=2.5e-3, width=1e-3)
+        U = cases.bubble_ic(c, a["cellCenter"], R0=2.5e-3, width=1e-3, u_wall=-20.0)
     elif ic == "tgv":
         U = cases.tgv_ic(c, a["cellCenter"])
     else:

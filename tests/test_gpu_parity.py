@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from conftest import rate_err, rel_err, state_err
-from gpu_cases import MIXED_TOL_SCALE, NAMES, make
+from gpu_cases import NAMES, case_tol, make
 from oracle.oracle_py import Oracle
 from fooskagpu_b200.api import Solver
 
@@ -31,8 +31,7 @@ REPORT = os.environ.get("FG_PARITY_REPORT")
 
 
 def _tol(name, prec):
-    f = MIXED_TOL_SCALE.get(name, 1.0) if prec == "mixed" else 1.0
-    return {k: v * f for k, v in TOL[prec].items()}
+    return case_tol(name, prec, TOL[prec])
 
 
 def _report(key, val):

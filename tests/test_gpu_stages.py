@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import rate_err, state_err
-from gpu_cases import MIXED_TOL_SCALE, NAMES, make
+from gpu_cases import NAMES, case_tol, make
 from oracle.oracle_py import Oracle
 from fooskagpu_b200.api import Solver
 
@@ -55,6 +55,6 @@ def test_one_step(name, prec, mode, meshdir):
     e = rate_err(Ug - U, Uo - U, U)  # the increments
     e_abs = state_err(Ug, Uo)
     _report(f"one_step/{name}/{prec}/{mode}", dict(incr=e.tolist(), state=e_abs.tolist()))
-    tol = TOL[prec] * (MIXED_TOL_SCALE.get(name, 1.0) if prec == "mixed" else 1.0)
+    tol = case_tol(name, prec, {"state": TOL[prec]})["state"]
     assert e_abs.max() < tol, e_abs
     s.close()

@@ -1,0 +1,91 @@
+"""Long-run comparison with the reference's own CUDA build: tests/golden/long_tgv16_slip.npz holds
+the state of oracle/_ref/fooska_ref_dp (the reference sources compiled by oracle/build_ref.py, run
+on a B200 by tests/golden/make_golden.py long) after 10, 30 and 60 full explicitLoop steps of a
+16^3 slip-wall Taylor-Green vortex.  The oracle (CPU) and the device path (GPU, FP64 and mixed)
+run the same steps from the same state and are compared field by field, and on the kinetic
+energy history.
+
+The reference accumulates its face fluxes with atomics (order not fixed), and its thermal
+relaxation stops at an absolute tolerance (1e-2 Pa / 1e-2 K), so two correct FP64 runs part
+at round-off level and the TGV amplifies that (about 30x per 10 steps from step 20 at Mach 0.1):
+the field tolerance grows with the step count, the kinetic energy is compared at 1e-6."""
+import numpy as np
+import pytest
+
+from fooskagpu_b200 import cases, meshgen
+
+ROOT_GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden" / "long_tgv16_slip.npz"
+
+# per step count: relative L2 tolerance of every conserved field (FP64 paths), of the mixed path
+FIELD_TOL = {10: 1e-10, 30: 1e-8, 60: 1e-6}
+MIXED_TOL = {10: 1e-5, 30: 1e-4, 60: 1e-3}
+
+
+def _setup(meshdir):
+    import sys
+    sys.path.insert(0, str(ROOT_GOLDEN.parent))
+    from make_golden import centres_of, long_spec
+    m, c = long_spec()
+    path = str(meshdir / "long_tgv16_slip.neu")
+    meshgen.write_neu(path, m)
+    return path, c, cases.tgv_ic(c, centres_of(m))
+
+
+def _field_err(U, R):
+    out = []
+    mom = np.linalg.norm(R[:, 3:6])
+    for v in range(10):
+        n = mom if 3 <= v <= 5 else np.linalg.norm(R[:, v])
+        out.append(np.linalg.norm(U[:, v] - R[:, v]) / n if n > 0 else 0.0)
+    return np.array(out)
+
+
+def _ke(U, vol):
+    rho = U[:, 1] + U[:, 2]
+    return float((0.5 * (U[:, 3] ** 2 + U[:, 4] ** 2 + U[:, 5] ** 2) / rho * vol).sum() / vol.sum())
+
+
+def test_oracle_follows_the_reference_binary(meshdir):
+    from fooskagpu_b200.api import Mesh
+    from oracle.oracle_py import Oracle
+    g = np.load(ROOT_GOLDEN)
+    path, c, U = _setup(meshdir)
+    assert np.array_equal(U, g["ic"])
+    m = Mesh.load_neu(path, scale=1.0)
+    vol = m.arrays()["volume"]
+    o = Oracle(m.view(), c)
+    Uo = U.copy()
+    done = 0
+    for k in (10, 30, 60):
+        while done < k:
+            o.step(Uo)
+            done += 1
+        R = g[f"U{k}"]
+        e = _field_err(Uo, R)
+        assert e.max() < FIELD_TOL[k], (k, e)
+        assert abs(_ke(Uo, vol) / _ke(R, vol) - 1) < 1e-6, k
+        assert abs(o.time.value - float(g[f"time{k}"])) <= 1e-12 * float(g[f"time{k}"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_device_path_follows_the_reference_binary(prec, meshdir):
+    from fooskagpu_b200.api import Mesh, Solver
+    g = np.load(ROOT_GOLDEN)
+    path, c, U = _setup(meshdir)
+    m = Mesh.load_neu(path, scale=1.0)
+    vol = m.arrays()["volume"]
+    s = Solver(m, c, precision=prec)
+    s.set_state(U)
+    done = 0
+    tol = FIELD_TOL if prec == "fp64" else MIXED_TOL
+    for k in (10, 30, 60):
+        while done < k:
+            s.step()
+            done += 1
+        Ug = s.get_state()
+        R = g[f"U{k}"]
+        e = _field_err(Ug, R)
+        assert e.max() < tol[k], (k, e)
+        assert abs(_ke(Ug, vol) / _ke(R, vol) - 1) < (1e-6 if prec == "fp64" else 1e-4), k
+    s.close()
