@@ -355,11 +355,12 @@ def bubble(args, torch, stream, dev):
       - mixed precision with the Newton;
       - mixed precision with the learned surrogate, trained here on the logged states.
     Every step is timed by CUDA events; between steps (outside the timed regions) fg_probe gives
-    the vapour volume and the pressure extrema.  The collapse time is the first time the vapour
-    volume falls below 10 % of its initial value (linear between steps); the peak pressure is the
-    largest mixture pressure seen up to 20 steps after it.  The FP64 run stops there (or after
-    FG_BENCH_BALL_STEPS steps); the two mixed runs take exactly as many steps, so their final
-    states are compared with the FP64 one.
+    the vapour volume and the pressure extrema.  The collapse time is the time of the vapour
+    volume's minimum; the peak pressure is the largest mixture pressure within 20 steps of it.  The
+    FP64 run stops 10 steps after the rebound (the vapour volume, below half its initial value, back
+    30 % above its minimum) or after FG_BENCH_BALL_STEPS steps; the two mixed runs take exactly as
+    many steps, and their density and pressure fields at mid-collapse (half that step count) are
+    compared with the FP64 run's.
     The limiter is the reference's (limiter = 0): with the van Albada-type extension the vapour
     partial density of interface cells turns negative within about 60 steps at 0.1 mm spacing,
     in the oracle as on the GPU, at any CFL number tried (0.5, 0.25); the parity tests cover that
@@ -384,7 +385,7 @@ def bubble(args, torch, stream, dev):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
-    def run(prec, nsteps, sg=None, log=0, stop_after_collapse=False):
+    def run(prec, nsteps, sg=None, log=0, stop_after_rebound=False, mid=None):
         s = Solver(mesh, case, precision=prec, device=dev)
         s.set_state(U0)
         if log:
@@ -392,14 +393,10 @@ def bubble(args, torch, stream, dev):
         if sg is not None:
             s.set_surrogate(sg, 1e-6, 3)
         v0 = s.probe()["vapourVolume"]
-        hist, ms, tc, pk, failed = [], 0.0, None, 0.0, None
+        hist, ms, failed, Umid = [], 0.0, None, None
         chem = fall = iters = relaxed = 0
-        after = 0
+        vmin, after = v0, -1
         for k in range(nsteps):
-            if stop_after_collapse and tc is not None:
-                after += 1
-                if after > 20:
-                    break
             e0.record(stream)
             try:
                 s.step(stream=stream.cuda_stream)
@@ -415,14 +412,19 @@ def bubble(args, torch, stream, dev):
             fall += st["nFallback"]
             iters += st["nIter"]
             relaxed += st["nChem"] + st["nTherm"]
-            t = s.time()[1]
-            if tc is None or after <= 20:
-                pk = max(pk, pr["maxPressure"])
-            if tc is None:
-                if hist and pr["vapourVolume"] < 0.1 * v0:
-                    tp, vp = hist[-1][0], hist[-1][1]
-                    tc = tp + (t - tp) * (vp - 0.1 * v0) / (vp - pr["vapourVolume"])
-            hist.append((t, pr["vapourVolume"], pr["maxPressure"]))
+            hist.append((s.time()[1], pr["vapourVolume"], pr["maxPressure"]))
+            if mid is not None and k + 1 == mid:
+                Umid = s.get_state()
+            vmin = min(vmin, pr["vapourVolume"])
+            if stop_after_rebound:
+                # the first collapse is over once the vapour volume, below half its initial
+                # value, has risen 30 % above its minimum; 10 more steps, then stop
+                if after < 0 and vmin < 0.5 * v0 and pr["vapourVolume"] > 1.3 * vmin:
+                    after = 0
+                elif after >= 0:
+                    after += 1
+                    if after >= 10:
+                        break
         try:
             s.check_state()
         except Exception as e:                # noqa: BLE001
@@ -431,21 +433,36 @@ def bubble(args, torch, stream, dev):
         data = s.relax_log_read(log) if log else None
         s.close()
         done = len(hist)
-        return dict(ms=ms, steps=done, U=U, hist=hist, tc=tc, peak=pk, failed=failed, chem=chem, fall=fall,
-                    iters_per_cell=iters / max(1, relaxed), data=data, v0=v0)
+        # collapse: the vapour volume's minimum (time of the step), and the largest mixture pressure
+        # within 20 steps of it
+        tc = pk = None
+        if done:
+            kmin = min(range(done), key=lambda q: hist[q][1])
+            if hist[kmin][1] < 0.5 * v0:
+                tc = hist[kmin][0]
+                pk = max(h[2] for h in hist[max(0, kmin - 20):kmin + 21])
+        return dict(ms=ms, steps=done, U=U, Umid=Umid, hist=hist, tc=tc, peak=pk, failed=failed, chem=chem,
+                    fall=fall, iters_per_cell=iters / max(1, relaxed), data=data, v0=v0,
+                    vmin_ratio=min((h[1] for h in hist), default=v0) / v0)
 
     def summary(r):
         out = {"value": nE * case.rkSteps * r["steps"] / (r["ms"] / 1e3), "steps_run": r["steps"],
                "collapse_time_s": r["tc"], "peak_pressure_pa": r["peak"],
+               "min_vapour_volume_over_initial": r["vmin_ratio"],
                "chem_cells_per_step": r["chem"] / max(1, r["steps"]),
                "newton_iters_per_relaxed_cell": r["iters_per_cell"]}
         if r["failed"]:
             out["stopped"] = r["failed"][:200]
         return out
 
-    r64 = run("fp64", steps, log=12_000_000, stop_after_collapse=True)
+    r64 = run("fp64", steps, log=12_000_000, stop_after_rebound=True)
     steps = r64["steps"]
+    mid = steps // 2
     res["steps"] = steps
+    # the FP64 run's mid-collapse state, for the density / pressure comparison
+    r64["Umid"] = None
+    rerun = run("fp64", mid, mid=mid)
+    r64["Umid"] = rerun["Umid"]
     X, Y = r64.pop("data")
     res["fp64"] = summary(r64)
     g = Surrogate(device=dev, seed=1)
@@ -457,9 +474,9 @@ def bubble(args, torch, stream, dev):
     res["surrogate_training"] = {"samples": take, "logged": int(len(X)), "epochs": epochs, "final_loss": loss,
                                  "seconds": time.perf_counter() - t0}
     del X, Y
-    rm = run("mixed", steps)
+    rm = run("mixed", steps, mid=mid)
     res["mixed"] = summary(rm)
-    rs = run("mixed", steps, sg=g)
+    rs = run("mixed", steps, sg=g, mid=mid)
     res["mixed_surrogate"] = summary(rs)
     res["value"] = res["mixed_surrogate"]["value"]
     res["fp64_value"] = res["fp64"]["value"]
@@ -469,19 +486,20 @@ def bubble(args, torch, stream, dev):
     res["history_fp64"] = {"every": 50, "t_s": [h[0] for h in r64["hist"][::50]],
                            "vapour_volume": [h[1] for h in r64["hist"][::50]],
                            "max_pressure": [h[2] for h in r64["hist"][::50]], "initial_vapour_volume": r64["v0"]}
-    # accuracy of the fast paths against the FP64 Newton run: the same number of steps
-    acc = {}
+    # accuracy of the fast paths against the FP64 Newton run: the density / pressure fields at
+    # mid-collapse (the same step), the collapse time and the peak pressure
+    acc = {"compared_at_step": mid}
     for key, r in (("mixed", rm), ("mixed_surrogate", rs)):
         e = {}
-        if r["steps"] == r64["steps"]:
-            fe = field_errors(case, r["U"], r64["U"])
+        if r["Umid"] is not None and r64["Umid"] is not None:
+            fe = field_errors(case, r["Umid"], r64["Umid"])
             e = {k: fe[k] for k in ("rho", "p") if k in fe}
         if r["tc"] is not None and r64["tc"] is not None:
             e["collapse_time_rel_err"] = abs(r["tc"] - r64["tc"]) / r64["tc"]
-        if r64["peak"] > 0:
+        if r["peak"] is not None and r64["peak"]:
             e["peak_pressure_rel_err"] = abs(r["peak"] - r64["peak"]) / r64["peak"]
         acc[key] = e
-    acc["tolerance"] = {"rel_l2": 1e-4, "note": "rho / p relative L2 after the run against the FP64 Newton run"}
+    acc["tolerance"] = {"rel_l2": 1e-4, "note": "rho / p relative L2 against the FP64 Newton run at the same step"}
     res["accuracy_vs_fp64"] = acc
     mesh.close()
     return res, g
@@ -606,9 +624,10 @@ def field_errors(case, U, Uref) -> dict:
 
 
 # tolerances of the accuracy checks (relative L2 / Linf per field against the FP64 oracle): the
-# FP64 path differs from the oracle by summation order and FMA contraction; the mixed path by its
-# FP32 face math (~1e-7 relative per stage)
-ACC_TOL = {"fp64": {"rel_l2": 1e-9, "rel_linf": 1e-6}, "mixed": {"rel_l2": 1e-5, "rel_linf": 1e-4}}
+# FP64 path differs from the oracle by summation order and FMA contraction, amplified where the
+# thermal Newton's absolute stopping tolerance (1e-2 Pa / 1e-2 K) changes a cell's iteration
+# count; the mixed path by its FP32 face math (~1e-7 relative per stage)
+ACC_TOL = {"fp64": {"rel_l2": 1e-8, "rel_linf": 1e-6}, "mixed": {"rel_l2": 1e-5, "rel_linf": 1e-4}}
 
 
 def accuracy(mesh, case, U0, Uref, steps, dev, torch, stream) -> dict:

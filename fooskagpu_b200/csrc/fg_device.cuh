@@ -251,8 +251,13 @@ __device__ __forceinline__ void hllc_flux(const PhysT<T> &P, const T *L, const T
 
 // WALE eddy viscosity (DP/computeViscousStresses.cu:3-60) for g = grad u (row i = component);
 // lsSq = Ls^2 = (0.325 Vavg^0.3333333333333)^2, precomputed per face on the host in FP64.
+// Without the constants 1e-12 and 1e-10 the formula is homogeneous of degree 1 in g, and
+// (S_d:S_d)^1.5 grows as |g|^6: in FP32 it overflows for gradients above about 1e6 1/s (a 200 m/s
+// jet over a 10 um cell).  For |g|max = lam > 1 the FP32 path therefore evaluates it on g / lam
+// with the constants divided by lam^5 and multiplies the result by lam: the same value in exact
+// arithmetic.  The FP64 path evaluates the reference's expression as written.
 template <typename T>
-__device__ __forceinline__ T wale_nu(const T *g, T lsSq) {
+__device__ __forceinline__ T wale_nu_scaled(const T *g, T lsSq, T eps, T zeroBelow) {
     T sq[9];
 #pragma unroll
     for (int i = 0; i < 3; i++)
@@ -271,9 +276,26 @@ __device__ __forceinline__ T wale_nu(const T *g, T lsSq) {
         }
     const T r1 = sqrt(s1), r2 = sqrt(s2);
     T num = s1 * r1;                       // s1^1.5
-    const T den = s1 * sqrt(r1) + s2 * s2 * r2 + (T)1e-12;  // s1^1.25 + s2^2.5 + 1e-12
-    if (den < (T)1e-10) num = 0;
+    const T den = s1 * sqrt(r1) + s2 * s2 * r2 + eps;  // s1^1.25 + s2^2.5 + 1e-12
+    if (den < zeroBelow) num = 0;
     return lsSq * num / den;
+}
+template <typename T>
+__device__ __forceinline__ T wale_nu(const T *g, T lsSq) {
+    return wale_nu_scaled(g, lsSq, (T)1e-12, (T)1e-10);
+}
+template <>
+__device__ __forceinline__ float wale_nu<float>(const float *g, float lsSq) {
+    float lam = 0.f;
+#pragma unroll
+    for (int q = 0; q < 9; q++) lam = fmaxf(lam, fabsf(g[q]));
+    if (!(lam > 1.f)) return wale_nu_scaled(g, lsSq, 1e-12f, 1e-10f);
+    const float inv = 1.f / lam;
+    float gs[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) gs[q] = g[q] * inv;
+    const float l2 = lam * lam, l5 = l2 * l2 * lam;   // inf above ~5e7: the constants vanish
+    return lam * wale_nu_scaled(gs, lsSq, 1e-12f / l5, 1e-10f / l5);
 }
 
 }  // namespace fg

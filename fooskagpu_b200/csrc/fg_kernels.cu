@@ -135,6 +135,17 @@ __device__ __forceinline__ void stage_geometry(const DevMesh<T> &m, int lo, int 
 }
 
 // ------------------------------------------------------------------ gradient + limiter
+// limiter function of a face increment diff with num = w_max - w or w_min - w: the reference's
+// phi = num / (2 diff), or the van Albada-type extension phi(r) = (r^2 + r) / (r^2 + 1), r = num / diff
+template <typename T, int kLim>
+__device__ __forceinline__ T limiter_phi(T num, T diff) {
+    if (kLim == 1) {
+        const T r = num / diff;
+        return (r * r + r) / (r * r + 1);
+    }
+    return num / (2 * diff);
+}
+
 // kLim: 0 the reference's limiter function, 1 the van Albada-type extension (fg_case.limiter)
 template <typename T, int kLim>
 __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_grad(const DevMesh<T> m, const T *__restrict__ W,
@@ -215,29 +226,32 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     const T iv = (T)(1.0 / m.vol[c]);
 #pragma unroll
     for (int q = 0; q < NP * 3; q++) gs[q] *= iv;
-    // limiter (DP/computeFaceValues.cu:66-81): theta = min over faces of clamp(phi, 0, 1)
-    T th[NP];
+    // limiter (DP/computeFaceValues.cu:66-81): theta = min over the faces of clamp(phi, 0, 1), phi
+    // of the face's increment diff = (w + (x_f - x_c) . grad w) - w and of num = w_max - w (diff
+    // > 0) or w_min - w (diff < 0).  clamp(phi) does not increase with |diff| on either side
+    // (for both limiter functions and either sign of num), so the minimum over the faces is that
+    // of the largest positive and of the most negative increment: two divisions per variable
+    // instead of one per face, the same result.
+    T dpos[NP], dneg[NP];
 #pragma unroll
-    for (int v = 0; v < NP; v++) th[v] = (T)1e9;
+    for (int v = 0; v < NP; v++) dpos[v] = dneg[v] = 0;
     for (int k = 0; k < nf; k++) {
         const T dx = geo.get(3, k), dy = geo.get(4, k), dz = geo.get(5, k);
 #pragma unroll
         for (int v = 0; v < NP; v++) {
             const T ext = dx * gs[3 * v] + dy * gs[3 * v + 1] + dz * gs[3 * v + 2];
-            const T wun = w[v] + ext;
-            const T diff = wun - w[v];
-            T phi = 1;
-            if (diff != 0) {
-                if (kLim == 1) {
-                    // van Albada-type limiter function (extension)
-                    const T r = ((wun > w[v]) ? (mx[v] - w[v]) : (mn[v] - w[v])) / diff;
-                    phi = (r * r + r) / (r * r + 1);
-                } else {
-                    phi = ((wun > w[v]) ? (mx[v] - w[v]) : (mn[v] - w[v])) / (2 * diff);
-                }
-            }
-            th[v] = fmin(th[v], fmax((T)0, fmin(phi, (T)1)));
+            const T diff = (w[v] + ext) - w[v];
+            dpos[v] = fmax(dpos[v], diff);
+            dneg[v] = fmin(dneg[v], diff);
         }
+    }
+    T th[NP];
+#pragma unroll
+    for (int v = 0; v < NP; v++) {
+        T t = 1;
+        if (dpos[v] > 0) t = fmin(t, limiter_phi<T, kLim>(mx[v] - w[v], dpos[v]));
+        if (dneg[v] < 0) t = fmin(t, limiter_phi<T, kLim>(mn[v] - w[v], dneg[v]));
+        th[v] = fmax((T)0, t);
     }
     T out[GREC];
 #pragma unroll
