@@ -411,18 +411,23 @@ struct SolverT : public fg_solver {
             }
             flags[i] = fl;
         }
-        // faces in GPU order: by owner cell (renumbered), then owner slot, so the owners of
-        // consecutive faces are consecutive cells (a ghost owns the faces it shares with own cells
-        // where the whole mesh makes it the owner)
+        // faces in GPU order: tiles of kFaceTile consecutive owner cells (renumbered); within a
+        // tile by the owner's element-local face (slot), then by owner.  The lanes of a gather warp
+        // then read the records of the same local face of nearby cells from nearby positions, and
+        // the face kernel's lanes take nearby owners whose neighbours lie in one direction of a hex
+        // brick.  A ghost owns the faces it shares with own cells where the whole mesh makes it the
+        // owner.
         std::vector<int32_t> gFace(nF, -1), slotFace(S, -1), fIdx(2 * (size_t)nF);
         int nG = 0;
-        for (int i = 0; i < n; i++) {
-            const int o = m.new2old[i];
-            const int nfc = fg::elem_type_for_nodes(m.elNN[o])->nFaces;
-            for (int k = 0; k < nfc; k++) {
-                const int f = elFc2fc[(size_t)o * 6 + k];
-                if (f >= 0 && elFcSide[(size_t)o * 6 + k] == 0) gFace[f] = nG++;
-            }
+        for (int t0 = 0; t0 < n; t0 += kFaceTile) {
+            const int t1 = std::min(n, t0 + kFaceTile);
+            for (int k = 0; k < MAXSLOT; k++)
+                for (int i = t0; i < t1; i++) {
+                    const int o = m.new2old[i];
+                    if (k >= fg::elem_type_for_nodes(m.elNN[o])->nFaces) continue;
+                    const int f = elFc2fc[(size_t)o * 6 + k];
+                    if (f >= 0 && elFcSide[(size_t)o * 6 + k] == 0) gFace[f] = nG++;
+                }
         }
         if (nG != nF) return set_err(FG_ERR_MESH, "internal: face ownership does not cover every face");
         // face geometry: 11 components (n[3], A, x_f - x_owner [3], x_f - x_nb [3], WALE Ls^2)
