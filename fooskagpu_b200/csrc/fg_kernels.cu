@@ -287,7 +287,7 @@ __device__ __forceinline__ void cell_grad_t(const PhysT<T> &P, const T *w, const
 // p1: neighbour state for the viscous flux (the cell-centre ghost on a boundary face);
 // gO / gN: the two cells' velocity gradients; gT: sum of their temperature gradients.
 template <typename T>
-__device__ __forceinline__ void face_tail(const PhysT<T> &P, const T *sL, const T *sR, const T *p1, const T *gO,
+__device__ __forceinline__ T face_tail(const PhysT<T> &P, const T *sL, const T *sR, const T *p1, const T *gO,
                                           const T *gN, const T *gT, int nb, T nx, T ny, T nz, T A, T lsSq,
                                           int wantSignal, T *__restrict__ FB, int fi) {
     T F[NV], unc, pF;
@@ -336,6 +336,17 @@ __device__ __forceinline__ void face_tail(const PhysT<T> &P, const T *sL, const 
     rec[NV] = A * unc;
     rec[NV + 1] = sig;
     store_frec(FB, fi, rec);
+    return sig;
+}
+
+// running maximum of a cell's face signal speeds: signal speeds are non-negative, and the integer
+// order of non-negative IEEE values is their numeric order, so the maximum is exact and independent
+// of the order of the updates.  A NaN signal is skipped, as fmax skips it.
+__device__ __forceinline__ void signal_max(float *a, float v) {
+    if (v >= 0.0f) atomicMax(reinterpret_cast<int *>(a), __float_as_int(v));
+}
+__device__ __forceinline__ void signal_max(double *a, double v) {
+    if (v >= 0.0) atomicMax(reinterpret_cast<long long *>(a), __double_as_longlong(v));
 }
 
 // ------------------------------------------------------------------ face flux (once per face)
@@ -349,7 +360,7 @@ __device__ __forceinline__ void face_tail(const PhysT<T> &P, const T *sL, const 
 //   momentum: -pC_c s A n summed = pC_c * (sum of outward n A)  (DP/flux.h:1-30, DP/computeRHS.cu:38-75)
 template <typename T>
 __global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
-                                              T *__restrict__ FB, const PhysT<T> P, int wantSignal) {
+                                              T *__restrict__ FB, T *cellSig, const PhysT<T> P, int wantSignal) {
     const int fi = blockIdx.x * blockDim.x + threadIdx.x;
     if (fi >= m.nF) return;
     const int o = m.fOwn[fi];
@@ -390,7 +401,12 @@ __global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(co
 #pragma unroll
         for (int q = 0; q < 9; q++) gN[q] = gO[q];
     }
-    face_tail(P, sL, sR, p1, gO, gN, gT, nb, nx, ny, nz, A, m.fLsSq[fi], wantSignal, FB, fi);
+    const T sig = face_tail(P, sL, sR, p1, gO, gN, gT, nb, nx, ny, nz, A, m.fLsSq[fi], wantSignal, FB, fi);
+    if (wantSignal == 2) {
+        // own cells only: a ghost's dt bound belongs to its own part
+        if (o < m.nU) signal_max(cellSig + o, sig);
+        if (nb >= 0 && nb < m.nU) signal_max(cellSig + nb, sig);
+    }
 }
 
 // ------------------------------------------------------------------ owner-side gather + RK
@@ -479,6 +495,30 @@ __global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gat
             for (int i = 1; i < (int)(blockDim.x >> 5); i++) bm = fmin(bm, red[i]);
             f.blockMin[blockIdx.x] = bm;
         }
+    }
+}
+
+// CFL bound of the own cells from their maximum face signal speed (k_face with wantSignal 2), as
+// the gather kernel computes it on the residual path: signal[c], then the deterministic block
+// minimum of volP / signal over blocks of the gather kernel's size
+template <typename T>
+__global__ void k_cell_cfl(const DevMesh<T> m, const T *__restrict__ cellSig, double *signal, double *blockMin) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double cfl = 1e12;
+    if (c < m.nU) {
+        const T sig = cellSig[c];
+        signal[c] = (double)sig;
+        cfl = m.volP[c] / (double)sig;
+    }
+    __shared__ double red[32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cfl = fmin(cfl, __shfl_down_sync(0xffffffffu, cfl, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cfl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double bm = red[0];
+        for (int i = 1; i < (int)(blockDim.x >> 5); i++) bm = fmin(bm, red[i]);
+        blockMin[blockIdx.x] = bm;
     }
 }
 
@@ -746,7 +786,12 @@ void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cud
 }
 template <typename T>
 void launch_face(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, int wantSignal, cudaStream_t s) {
-    k_face<T><<<(m.nF + FG_FACE_THREADS - 1) / FG_FACE_THREADS, FG_FACE_THREADS, 0, s>>>(m, f.Win, f.G, f.FB, P, wantSignal);
+    k_face<T><<<(m.nF + FG_FACE_THREADS - 1) / FG_FACE_THREADS, FG_FACE_THREADS, 0, s>>>(m, f.Win, f.G, f.FB, f.cellSig, P,
+                                                                                      wantSignal);
+}
+template <typename T>
+void launch_cell_cfl(const DevMesh<T> &m, const Fields<T> &f, cudaStream_t s) {
+    k_cell_cfl<T><<<flux_blocks(m.nU), kGatherThreads, 0, s>>>(m, f.cellSig, f.signal, f.blockMin);
 }
 template <typename T>
 void launch_gather(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, int mode, int wantSignal,
@@ -812,6 +857,8 @@ template void launch_grad<float>(const DevMesh<float> &, const Fields<float> &, 
 template void launch_grad<double>(const DevMesh<double> &, const Fields<double> &, const PhysT<double> &, cudaStream_t);
 template void launch_face<float>(const DevMesh<float> &, const Fields<float> &, const PhysT<float> &, int, cudaStream_t);
 template void launch_face<double>(const DevMesh<double> &, const Fields<double> &, const PhysT<double> &, int, cudaStream_t);
+template void launch_cell_cfl<float>(const DevMesh<float> &, const Fields<float> &, cudaStream_t);
+template void launch_cell_cfl<double>(const DevMesh<double> &, const Fields<double> &, cudaStream_t);
 template void launch_gather<float>(const DevMesh<float> &, const Fields<float> &, const PhysD &, int, int, StageCoef, cudaStream_t);
 template void launch_gather<double>(const DevMesh<double> &, const Fields<double> &, const PhysD &, int, int, StageCoef, cudaStream_t);
 template void launch_update<float>(const DevMesh<float> &, const Fields<float> &, const PhysD &, StageCoef, cudaStream_t);

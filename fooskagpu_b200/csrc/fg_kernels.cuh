@@ -117,6 +117,7 @@ struct Fields {
     T *Wout;            // primitive records written this stage
     T *G;               // limiter + gradient records (GREC values per cell, component-major)
     double *signal;     // [n]
+    T *cellSig;         // [n] per-cell maximum face signal speed of a dt step (zeroed before it)
     double *blockMin;   // [nBlocks]
     double *dt;         // device scalar
     int32_t *bad;       // set to the step counter + 1 when an updated state is not finite or its
@@ -147,6 +148,8 @@ void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cud
 // one-time kernel attribute set-up (dynamic shared memory above 48 KB)
 template <typename T>
 int stage_kernels_setup(const DevMesh<T> &m);
+// wantSignal: 0 none; 1 the face signal speeds into the face records; 2 also their per-cell maxima
+// into Fields::cellSig
 template <typename T>
 void launch_face(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, int wantSignal, cudaStream_t s);
 template <typename T>
@@ -163,6 +166,10 @@ template <typename T>
 void launch_halo_pack(const T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, T *out, cudaStream_t s);
 template <typename T>
 void launch_halo_unpack(T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, const T *in, cudaStream_t s);
+// dt steps of the fused path: per cell (own cells, blocks of the gather kernel) the CFL bound
+// volP / cellSig and the signal, the block minima into blockMin[flux_blocks(nU)]
+template <typename T>
+void launch_cell_cfl(const DevMesh<T> &m, const Fields<T> &f, cudaStream_t s);
 // dt = min(cfl * min_blocks, maxDt) from blockMin[nBlocks]
 void launch_dt_finalize(const double *blockMin, int nBlocks, double cfl, double maxDt, double *dt, cudaStream_t s);
 int flux_blocks(int n);   // blocks of the gather kernel (= entries of blockMin)

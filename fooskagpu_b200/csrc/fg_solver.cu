@@ -192,6 +192,8 @@ struct fg_solver {
     // download U; wait = false leaves the copy queued on the stream
     virtual int get_state(double *U, cudaStream_t s, bool wait) = 0;
     virtual int compute_rhs(int wantSignal, cudaStream_t s) = 0;
+    // stage irk with a new dt first (the dt step of explicitLoop), fused
+    virtual int dt_stage(int irk, int writeU0, cudaStream_t s) = 0;
     virtual int time_step(double *dtOut, cudaStream_t s) = 0;
     virtual int init_rk(cudaStream_t s) = 0;
     virtual int update(int irk, int writeU0, cudaStream_t s) = 0;
@@ -256,7 +258,7 @@ __global__ void k_field_vars(int n, const double *__restrict__ U, const T *__res
 template <typename T>
 struct SolverT : public fg_solver {
     DevBuf dNbr, dFlags, dGeo, dVol, dVolP, dNew2Old, dHaloStart, dHaloIds, dSlotLocal;
-    DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dBlockMin, dScal, dCnt, dCons, dStage;
+    DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dCellSig, dBlockMin, dScal, dCnt, dCons, dStage;
     DevBuf dStageIn;   // staging buffer of the asynchronous uploads (on first use)
     DevBuf dFIdx, dFGeo, dSlotFace, dClosure, dFB;
     DevBuf dOrdFlag, dOrdCnt, dOrdOff, dOrder, dOrdTotal;   // relaxation cell ordering
@@ -281,6 +283,7 @@ struct SolverT : public fg_solver {
         f.Wout = dW[1 - wIn].as<T>();
         f.G = dG.as<T>();
         f.signal = dSig.as<double>();
+        f.cellSig = dCellSig.as<T>();
         f.blockMin = dBlockMin.as<double>();
         f.dt = dScal.as<double>();
         f.bad = dBad;
@@ -550,6 +553,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dW[1].alloc((size_t)n * WREC * sizeof(T)));
         FG_CUDA_TRY(dG.alloc((size_t)n * GREC * sizeof(T)));
         FG_CUDA_TRY(dSig.alloc((size_t)n * sizeof(double)));
+        FG_CUDA_TRY(dCellSig.alloc((size_t)n * sizeof(T)));
         FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n), cons_blocks(n)) * sizeof(double)));
         FG_CUDA_TRY(dScal.alloc(4 * sizeof(double)));   // dt, time, cons
         FG_CUDA_TRY(dCnt.alloc(8 * sizeof(int32_t)));
@@ -573,7 +577,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(cudaMemcpy(dScal.p, scal, sizeof(scal), cudaMemcpyHostToDevice));
         bytes = 0;
         for (DevBuf *b : {&dNbr, &dFlags, &dGeo, &dVol, &dVolP, &dNew2Old, &dU, &dU0, &dRHS, &dStage, &dW[0], &dW[1], &dG,
-                          &dSig, &dBlockMin, &dScal, &dCnt, &dHaloStart, &dHaloIds, &dSlotLocal, &dFIdx, &dFGeo,
+                          &dSig, &dCellSig, &dBlockMin, &dScal, &dCnt, &dHaloStart, &dHaloIds, &dSlotLocal, &dFIdx, &dFGeo,
                           &dSlotFace, &dClosure, &dFB, &dOrdFlag, &dOrdCnt, &dOrdOff, &dOrder, &dOrdTotal,
                           &dPred, &dHullOk, &dTcErr})
             bytes += b->bytes;
@@ -768,6 +772,29 @@ struct SolverT : public fg_solver {
         launch_update<T>(dm, f, D, coef(irk, writeU0), s);
         prof_end(s);
         FG_LAUNCH_CHECK("update");
+        cur ^= 1;
+        return FG_OK;
+    }
+    int dt_stage(int irk, int writeU0, cudaStream_t s) override {
+        // the face kernel also keeps each cell's maximum face signal, so the new dt is known before
+        // the fused gather + RK update of this stage (no residual buffer, no separate update pass);
+        // dt, signal and the updated state equal those of compute_rhs + time_step + update
+        int rc;
+        if ((rc = gradients_halo(s))) return rc;
+        Fields<T> f = fields(cur);
+        FG_CUDA_TRY(cudaMemsetAsync(dCellSig.p, 0, (size_t)n * sizeof(T), s));
+        prof_begin(FG_K_FLUX, s);
+        launch_face<T>(dm, f, P, 2, s);
+        prof_end(s);
+        prof_begin(FG_K_DT, s);
+        launch_cell_cfl<T>(dm, f, s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("cell cfl");
+        if ((rc = time_step(nullptr, s))) return rc;
+        prof_begin(FG_K_GATHER, s);
+        launch_gather<T>(dm, f, D, FLUX_FUSED, 0, coef(irk, writeU0), s);
+        prof_end(s);
+        FG_LAUNCH_CHECK("dt stage");
         cur ^= 1;
         return FG_OK;
     }
@@ -1393,9 +1420,7 @@ int fg_step(fg_solver *s, void *stream) {
         const int writeU0 = (rk == 3 && irk == 0);
         if (c.adaptDt == 1 && irk == 0 && s->iStep % c.adaptDtItr == 0) {
             // residual with the signal speeds, new dt, then the stage update (DP/explicitLoop.cu:45-47)
-            if ((rc = s->compute_rhs(1, st))) return rc;
-            if ((rc = s->time_step(nullptr, st))) return rc;
-            if ((rc = s->update(irk, writeU0, st))) return rc;
+            if ((rc = s->dt_stage(irk, writeU0, st))) return rc;
         } else {
             if ((rc = s->stage(irk, writeU0, st))) return rc;
         }

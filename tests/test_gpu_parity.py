@@ -227,6 +227,37 @@ def test_periodic_conservation(prec, meshdir):
     s.close()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["mixed_ref_rk3", "tet_ext", "hex_periodic_tgv"])
+def test_dt_step_matches_stage_api(name, prec, meshdir):
+    """A step that computes a new dt (fg_step: the face kernel keeps each cell's maximum face
+    signal speed, then the fused gather + RK update) equals fg_init_rk + fg_compute_rhs with the
+    signal + fg_compute_time_step + fg_update for its first stage and fg_stage for the others,
+    bit for bit: dt, per-cell signal and state."""
+    m, c, U = make(name, meshdir, prec)
+    c.adaptDt = 1
+    c.adaptDtItr = 1
+    c.relaxFlag = 1
+    c.consCalcFlag = 0
+    a = Solver(m, c, precision=prec)
+    b = Solver(m, c, precision=prec)
+    a.set_state(U)
+    b.set_state(U)
+    for _ in range(2):
+        a.step()
+        b.init_rk()
+        b.compute_rhs(want_signal=True)
+        dt = b.compute_time_step()
+        b.update(0)
+        for irk in range(1, c.rkSteps):
+            b.stage(irk)
+        assert a.time()[0] == dt
+        assert np.array_equal(a.get_signal(), b.get_signal())
+        assert np.array_equal(a.get_state(), b.get_state())
+    a.close()
+    b.close()
+
+
 def test_stage_api_matches_step(meshdir):
     """fg_init_rk + fg_compute_rhs + fg_update per stage equals the fused fg_stage path."""
     m, c, U = make("mixed_ref_rk3", meshdir)
