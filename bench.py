@@ -349,8 +349,8 @@ def bubble(args, torch, stream, dev):
     a ball of radius 10 R0 = 10 mm, about 4 M tets graded toward the centre (meshgen.ball_tets,
     built in memory with the GPU pre-processor), a vapour bubble of R0 = 1 mm at 2340 Pa in water at
     10 MPa (Rayleigh-Plesset pressure field, 298.15 K), stiffened-gas water / vapour constants
-    (cases.water_vapour_constants), Gibbs-equilibrium Newton relaxation, HLLC + MUSCL with the van
-    Albada-type limiter, SSP-RK3.  Three runs of the same `steps` steps from the same state:
+    (cases.water_vapour_constants), Gibbs-equilibrium Newton relaxation, HLLC + MUSCL with the
+    reference's limiter (below), SSP-RK3.  Three runs of the same `steps` steps from the same state:
       - FP64 with the reference Newton, logging the converged chemical solves (training data);
       - mixed precision with the Newton;
       - mixed precision with the learned surrogate, trained here on the logged states.
@@ -359,8 +359,12 @@ def bubble(args, torch, stream, dev):
     volume's minimum; the peak pressure is the largest mixture pressure within 20 steps of it.  The
     FP64 run stops 10 steps after the rebound (the vapour volume, below half its initial value, back
     30 % above its minimum) or after FG_BENCH_BALL_STEPS steps; the two mixed runs take exactly as
-    many steps, and their density and pressure fields at mid-collapse (half that step count) are
-    compared with the FP64 run's.
+    many steps.  Their density and pressure fields are compared with the FP64 run's at steps 100,
+    500 and 1000, and so are those of a fourth run, FP64 from the initial state perturbed by a seeded
+    relative 1e-10: the collapse is chaotic once the first interface cells cavitate (about step 200
+    at this resolution, the maximum pressure jumping from 9e6 to 2e8 Pa), after which FP64 itself
+    moves by 10-30 % in pressure L2 under that perturbation, so the tolerance applies at step 100
+    and the later steps are reported beside the perturbed FP64 run's divergence.
     The limiter is the reference's (limiter = 0): with the van Albada-type extension the vapour
     partial density of interface cells turns negative within about 60 steps at 0.1 mm spacing,
     in the oracle as on the GPU, at any CFL number tried (0.5, 0.25); the parity tests cover that
@@ -385,15 +389,17 @@ def bubble(args, torch, stream, dev):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
-    def run(prec, nsteps, sg=None, log=0, stop_after_rebound=False, mid=None):
+    compare = (100, 500, 1000)
+
+    def run(prec, nsteps, sg=None, log=0, stop_after_rebound=False, U_init=None):
         s = Solver(mesh, case, precision=prec, device=dev)
-        s.set_state(U0)
+        s.set_state(U0 if U_init is None else U_init)
         if log:
             s.relax_log(log)
         if sg is not None:
             s.set_surrogate(sg, 1e-6, 3)
         v0 = s.probe()["vapourVolume"]
-        hist, ms, failed, Umid = [], 0.0, None, None
+        hist, ms, failed, snaps = [], 0.0, None, {}
         chem = fall = iters = relaxed = 0
         vmin, after = v0, -1
         for k in range(nsteps):
@@ -413,8 +419,8 @@ def bubble(args, torch, stream, dev):
             iters += st["nIter"]
             relaxed += st["nChem"] + st["nTherm"]
             hist.append((s.time()[1], pr["vapourVolume"], pr["maxPressure"]))
-            if mid is not None and k + 1 == mid:
-                Umid = s.get_state()
+            if k + 1 in compare:
+                snaps[k + 1] = s.get_state()
             vmin = min(vmin, pr["vapourVolume"])
             if stop_after_rebound:
                 # the first collapse is over once the vapour volume, below half its initial
@@ -441,7 +447,7 @@ def bubble(args, torch, stream, dev):
             if hist[kmin][1] < 0.5 * v0:
                 tc = hist[kmin][0]
                 pk = max(h[2] for h in hist[max(0, kmin - 20):kmin + 21])
-        return dict(ms=ms, steps=done, U=U, Umid=Umid, hist=hist, tc=tc, peak=pk, failed=failed, chem=chem,
+        return dict(ms=ms, steps=done, U=U, snaps=snaps, hist=hist, tc=tc, peak=pk, failed=failed, chem=chem,
                     fall=fall, iters_per_cell=iters / max(1, relaxed), data=data, v0=v0,
                     vmin_ratio=min((h[1] for h in hist), default=v0) / v0)
 
@@ -457,12 +463,7 @@ def bubble(args, torch, stream, dev):
 
     r64 = run("fp64", steps, log=12_000_000, stop_after_rebound=True)
     steps = r64["steps"]
-    mid = steps // 2
     res["steps"] = steps
-    # the FP64 run's mid-collapse state, for the density / pressure comparison
-    r64["Umid"] = None
-    rerun = run("fp64", mid, mid=mid)
-    r64["Umid"] = rerun["Umid"]
     X, Y = r64.pop("data")
     res["fp64"] = summary(r64)
     g = Surrogate(device=dev, seed=1)
@@ -474,10 +475,15 @@ def bubble(args, torch, stream, dev):
     res["surrogate_training"] = {"samples": take, "logged": int(len(X)), "epochs": epochs, "final_loss": loss,
                                  "seconds": time.perf_counter() - t0}
     del X, Y
-    rm = run("mixed", steps, mid=mid)
+    rm = run("mixed", steps)
     res["mixed"] = summary(rm)
-    rs = run("mixed", steps, sg=g, mid=mid)
+    rs = run("mixed", steps, sg=g)
     res["mixed_surrogate"] = summary(rs)
+    # the sensitivity of the FP64 run itself: a seeded relative 1e-10 perturbation of the state
+    rng = np.random.default_rng(20261204)
+    Up = U0 * (1.0 + 1e-10 * rng.standard_normal(U0.shape))
+    Up[:, 0] = np.clip(Up[:, 0], 0.0, 1.0)
+    rp = run("fp64", min(steps, max(compare)), U_init=Up)
     res["value"] = res["mixed_surrogate"]["value"]
     res["fp64_value"] = res["fp64"]["value"]
     res["mixed_surrogate_over_fp64"] = res["value"] / res["fp64_value"]
@@ -486,20 +492,30 @@ def bubble(args, torch, stream, dev):
     res["history_fp64"] = {"every": 50, "t_s": [h[0] for h in r64["hist"][::50]],
                            "vapour_volume": [h[1] for h in r64["hist"][::50]],
                            "max_pressure": [h[2] for h in r64["hist"][::50]], "initial_vapour_volume": r64["v0"]}
-    # accuracy of the fast paths against the FP64 Newton run: the density / pressure fields at
-    # mid-collapse (the same step), the collapse time and the peak pressure
-    acc = {"compared_at_step": mid}
-    for key, r in (("mixed", rm), ("mixed_surrogate", rs)):
+    # accuracy of the fast paths against the FP64 Newton run: the density / pressure fields at the
+    # same steps, the collapse time and the peak pressure; beside them the divergence of the
+    # perturbed FP64 run (the problem's own sensitivity)
+    steps_cmp = [k for k in compare if k in r64["snaps"]]
+    acc = {"compared_at_steps": steps_cmp}
+    for key, r in (("mixed", rm), ("mixed_surrogate", rs), ("fp64_perturbed_1e-10", rp)):
         e = {}
-        if r["Umid"] is not None and r64["Umid"] is not None:
-            fe = field_errors(case, r["Umid"], r64["Umid"])
-            e = {k: fe[k] for k in ("rho", "p") if k in fe}
-        if r["tc"] is not None and r64["tc"] is not None:
-            e["collapse_time_rel_err"] = abs(r["tc"] - r64["tc"]) / r64["tc"]
-        if r["peak"] is not None and r64["peak"]:
-            e["peak_pressure_rel_err"] = abs(r["peak"] - r64["peak"]) / r64["peak"]
+        for k in steps_cmp:
+            if k in r["snaps"]:
+                fe = field_errors(case, r["snaps"][k], r64["snaps"][k])
+                e[f"step_{k}"] = {f: fe[f] for f in ("rho", "p") if f in fe}
+        if key != "fp64_perturbed_1e-10":
+            if r["tc"] is not None and r64["tc"] is not None:
+                e["collapse_time_rel_err"] = abs(r["tc"] - r64["tc"]) / r64["tc"]
+            if r["peak"] is not None and r64["peak"]:
+                e["peak_pressure_rel_err"] = abs(r["peak"] - r64["peak"]) / r64["peak"]
         acc[key] = e
-    acc["tolerance"] = {"rel_l2": 1e-4, "note": "rho / p relative L2 against the FP64 Newton run at the same step"}
+    tol_step = steps_cmp[0] if steps_cmp else None
+    acc["tolerance"] = {"rel_l2": 1e-4, "step": tol_step,
+                        "note": "rho / p relative L2 against the FP64 Newton run, before the first cavitation; later "
+                                "steps are chaotic and reported beside the 1e-10-perturbed FP64 run"}
+    if tol_step is not None:
+        acc["pass"] = {key: all(acc[key].get(f"step_{tol_step}", {}).get(f, {}).get("rel_l2", 1.0) <= 1e-4
+                                for f in ("rho", "p")) for key in ("mixed", "mixed_surrogate")}
     res["accuracy_vs_fp64"] = acc
     mesh.close()
     return res, g
