@@ -400,7 +400,7 @@ def bubble(args, torch, stream, dev):
             s.set_surrogate(sg, 1e-6, 3)
         v0 = s.probe()["vapourVolume"]
         hist, ms, failed, snaps = [], 0.0, None, {}
-        chem = fall = iters = relaxed = 0
+        chem = fall = iters = relaxed = acc_sg = polish = 0
         vmin, after = v0, -1
         for k in range(nsteps):
             e0.record(stream)
@@ -416,6 +416,8 @@ def bubble(args, torch, stream, dev):
             st = s.relax_stats()
             chem += st["nChem"]
             fall += st["nFallback"]
+            acc_sg += st["nSurrogate"]
+            polish += st["nPolish"]
             iters += st["nIter"]
             relaxed += st["nChem"] + st["nTherm"]
             hist.append((s.time()[1], pr["vapourVolume"], pr["maxPressure"]))
@@ -448,7 +450,8 @@ def bubble(args, torch, stream, dev):
                 tc = hist[kmin][0]
                 pk = max(h[2] for h in hist[max(0, kmin - 20):kmin + 21])
         return dict(ms=ms, steps=done, U=U, snaps=snaps, hist=hist, tc=tc, peak=pk, failed=failed, chem=chem,
-                    fall=fall, iters_per_cell=iters / max(1, relaxed), data=data, v0=v0,
+                    fall=fall, iters_per_cell=iters / max(1, relaxed), data=data, v0=v0, accepted=acc_sg,
+                    polish_per_accepted=polish / acc_sg if acc_sg else None,
                     vmin_ratio=min((h[1] for h in hist), default=v0) / v0)
 
     def summary(r):
@@ -489,6 +492,8 @@ def bubble(args, torch, stream, dev):
     res["mixed_surrogate_over_fp64"] = res["value"] / res["fp64_value"]
     res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64_value"]
     res["fallback_rate"] = rs["fall"] / max(1, rs["chem"])
+    res["surrogate_accepted_cells"] = rs["accepted"]
+    res["polish_steps_per_accepted_cell"] = rs["polish_per_accepted"]
     res["history_fp64"] = {"every": 50, "t_s": [h[0] for h in r64["hist"][::50]],
                            "vapour_volume": [h[1] for h in r64["hist"][::50]],
                            "max_pressure": [h[2] for h in r64["hist"][::50]], "initial_vapour_volume": r64["v0"]}

@@ -76,7 +76,7 @@ KERNEL_KINDS = ["grad", "flux", "update", "relax", "dt", "cons", "other", "gathe
 
 class FgRelaxStats(C.Structure):
     _fields_ = [("nTherm", i32), ("nChem", i32), ("nAbort", i32), ("nIter", i32), ("nSurrogate", i32),
-                ("nFallback", i32)]
+                ("nFallback", i32), ("nPolish", i32)]
 
 
 class FgPartitionInfo(C.Structure):

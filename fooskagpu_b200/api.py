@@ -246,7 +246,7 @@ class Solver:
         st = FgRelaxStats()
         check(lib().fg_relaxation(self._h, C.byref(st), stream))
         return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter,
-                "nSurrogate": st.nSurrogate, "nFallback": st.nFallback}
+                "nSurrogate": st.nSurrogate, "nFallback": st.nFallback, "nPolish": st.nPolish}
 
     def check_state(self) -> int:
         """-1 if the state is healthy; raises FgError (FG_ERR_NAN) naming the step otherwise."""
@@ -269,7 +269,7 @@ class Solver:
         st = FgRelaxStats()
         check(lib().fg_relax_stats_read(self._h, C.byref(st)))
         return {"nTherm": st.nTherm, "nChem": st.nChem, "nAbort": st.nAbort, "nIter": st.nIter,
-                "nSurrogate": st.nSurrogate, "nFallback": st.nFallback}
+                "nSurrogate": st.nSurrogate, "nFallback": st.nFallback, "nPolish": st.nPolish}
 
     # -- learned equilibrium surrogate
     def set_surrogate(self, sg: Optional["Surrogate"], rel_tol: float = 1e-6, polish_iters: int = 3) -> None:

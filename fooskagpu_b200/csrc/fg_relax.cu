@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBL
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool act = i < n;
     const int c = (kOrd && act) ? order[i] : i;
-    int chem = 0, ab = 0, its = 0, used = 0;
+    int chem = 0, ab = 0, its = 0, used = 0, pits = 0;
     const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
     double u[NV];
     double rm = 0, re = 0, ag = 0;
@@ -497,7 +497,6 @@ __global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBL
         }
     }
     if (act) {
-        int pits = 0;
         if (kSG && want) {
             const float4 p4 = pred[i];
             const float pr[4] = {p4.x, p4.y, p4.z, p4.w};
@@ -540,6 +539,7 @@ __global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBL
     const unsigned maskS = __ballot_sync(0xffffffffu, act && used);
     const unsigned maskF = __ballot_sync(0xffffffffu, act && chem && kSG && !used);
     const int itsW = __reduce_add_sync(0xffffffffu, its);
+    const int polW = kSG ? __reduce_add_sync(0xffffffffu, used ? pits : 0) : 0;   // polish steps of accepted cells
     if ((threadIdx.x & 31) == 0) {
         if (maskT) atomicAdd(&counters[0], __popc(maskT));
         if (mask) atomicAdd(&counters[1], __popc(mask));
@@ -547,6 +547,7 @@ __global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBL
         if (itsW) atomicAdd(&counters[3], itsW);
         if (maskS) atomicAdd(&counters[4], __popc(maskS));
         if (maskF) atomicAdd(&counters[5], __popc(maskF));
+        if (polW) atomicAdd(&counters[6], polW);
     }
 }
 

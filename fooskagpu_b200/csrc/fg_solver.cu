@@ -836,6 +836,7 @@ struct SolverT : public fg_solver {
         st->nIter = h[3];
         st->nSurrogate = h[4];
         st->nFallback = h[5];
+        st->nPolish = h[6];
         return FG_OK;
     }
     int probe(double *out4, cudaStream_t s) override {

@@ -310,6 +310,7 @@ typedef struct fg_relax_stats {
     int32_t nSurrogate;   /* chemical cells solved from the surrogate's prediction            */
     int32_t nFallback;    /* chemical cells that took the reference Newton with a surrogate attached
                              (outside the training hull, or polish residual above tolerance)   */
+    int32_t nPolish;      /* polish Newton steps of the cells counted in nSurrogate            */
 } fg_relax_stats;
 int fg_relaxation(fg_solver *s, fg_relax_stats *stats, void *stream);
 /* counts of the most recent relaxation, including the one inside fg_step (synchronises) */

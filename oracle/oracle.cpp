@@ -1098,7 +1098,7 @@ void orc_relaxation(const fg_case *c, const fg_mesh_view *m, double *U, fg_relax
         else { nA += therm_relax_cell(c, u, &it); nT++; }
         nI += it;
     }
-    if (st) { st->nTherm = nT; st->nChem = nC; st->nAbort = nA; st->nIter = nI; st->nSurrogate = 0; st->nFallback = 0; }
+    if (st) { st->nTherm = nT; st->nChem = nC; st->nAbort = nA; st->nIter = nI; st->nSurrogate = 0; st->nFallback = 0; st->nPolish = 0; }
 }
 
 /* integrateConsVar + consCalc (DP/consCalc.cu:3-60); fixed 4096-cell chunks so the result

@@ -142,6 +142,8 @@ def test_relaxation_gain_and_parity(box, trained):
     assert st1["nChem"] == st0["nChem"] > 1000 and st1["nTherm"] == st0["nTherm"]
     assert st1["nSurrogate"] + st1["nFallback"] == st1["nChem"]
     assert st1["nSurrogate"] > 0.9 * st1["nChem"], st1          # fallback rate below 10 %
+    # polish steps of the accepted cells: at least one each, at most the cap
+    assert st1["nSurrogate"] <= st1["nPolish"] <= POLISH * st1["nSurrogate"], st1
     assert st1["nIter"] < 0.5 * st0["nIter"], (st0, st1)         # the gain: Newton work halved at least
     assert d.max() < 1e-4, d
     s0.close()
@@ -164,6 +166,7 @@ def test_untrained_network_falls_back_to_newton(box, data):
     s1.set_surrogate(g, REL_TOL, 0)
     st1 = s1.relaxation()
     assert st1["nSurrogate"] == 0 and st1["nFallback"] == st1["nChem"] == st0["nChem"]
+    assert st1["nPolish"] == 0 and st0["nPolish"] == 0
     assert st1["nIter"] == st0["nIter"]
     assert np.array_equal(s1.get_state(), s0.get_state())
     s0.close()
