@@ -116,6 +116,7 @@ SIGNATURES = {
     "fg_set_state_async": (C.c_int, [VP, PD, VP]),
     "fg_get_state": (C.c_int, [VP, PD, VP]),
     "fg_get_state_async": (C.c_int, [VP, PD, VP]),
+    "fg_state_join": (C.c_int, [VP, VP]),
     "fg_compute_rhs": (C.c_int, [VP, i32, VP]),
     "fg_compute_time_step": (C.c_int, [VP, PD, VP]),
     "fg_init_rk": (C.c_int, [VP, VP]),

@@ -181,10 +181,16 @@ class Solver:
         check(lib().fg_set_state_async(self._h, _dptr(U), stream))
 
     def get_state_async(self, out: np.ndarray, stream: Optional[int] = None) -> None:
-        """Queue the download into `out` (fg_get_state_async); complete once the stream has passed it."""
+        """Queue the download into `out` (fg_get_state_async): the copy runs on the solver's
+        download stream; `out` is complete once a stream joined by state_join has passed that
+        point (or after a device synchronisation)."""
         if not (out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.shape == (self.n, 10)):
             raise ValueError("get_state_async needs a C-contiguous float64 array of shape (n, 10)")
         check(lib().fg_get_state_async(self._h, _dptr(out), stream))
+
+    def state_join(self, stream: Optional[int] = None) -> None:
+        """Make `stream` wait on the device for every get_state_async issued so far (fg_state_join)."""
+        check(lib().fg_state_join(self._h, stream))
 
     def get_state(self, out: Optional[np.ndarray] = None, stream: Optional[int] = None) -> np.ndarray:
         if out is None:

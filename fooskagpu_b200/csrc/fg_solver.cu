@@ -74,12 +74,27 @@ struct fg_solver {
         if (evInFree) cudaEventDestroy(evInFree);
         if (evCopied) cudaEventDestroy(evCopied);
         if (copyStream) cudaStreamDestroy(copyStream);
+        for (cudaEvent_t e : evOutFree)
+            if (e) cudaEventDestroy(e);
+        if (evGathered) cudaEventDestroy(evGathered);
+        if (downStream) cudaStreamDestroy(downStream);
     }
     // asynchronous uploads copy on their own stream into their own staging buffer, so the copy of
     // the next state overlaps the work queued before it (created on the first asynchronous upload)
     cudaStream_t copyStream = nullptr;
     cudaEvent_t evInFree = nullptr;   // the last scatter has read the upload staging buffer
     cudaEvent_t evCopied = nullptr;   // the upload copy has landed
+    // asynchronous downloads: the gather kernel on the caller's stream into one of two staging
+    // buffers, the copy to the host on the solver's download stream (created on first use)
+    cudaStream_t downStream = nullptr;
+    cudaEvent_t evOutFree[2] = {nullptr, nullptr};   // the download from staging buffer b has finished
+    cudaEvent_t evGathered = nullptr;                // the gather into the current buffer is done
+    int outNext = 0;                                 // staging buffer of the next download
+    int state_join(cudaStream_t s) {
+        // the download stream runs its copies in order: waiting for the last one covers all
+        if (downStream) FG_CUDA_TRY(cudaStreamWaitEvent(s, evOutFree[outNext ^ 1], 0));
+        return FG_OK;
+    }
     int init_flag() {
         void *h = nullptr;
         FG_CUDA_TRY(cudaHostAlloc(&h, 2 * sizeof(int32_t), cudaHostAllocMapped));
@@ -260,6 +275,7 @@ struct SolverT : public fg_solver {
     DevBuf dNbr, dFlags, dGeo, dVol, dVolP, dNew2Old, dHaloStart, dHaloIds, dSlotLocal;
     DevBuf dU, dU0, dRHS, dW[2], dG, dSig, dCellSig, dBlockMin, dScal, dCnt, dCons, dStage;
     DevBuf dStageIn;   // staging buffer of the asynchronous uploads (on first use)
+    DevBuf dStageOut[2];   // staging buffers of the asynchronous downloads (on first use)
     DevBuf dFIdx, dFGeo, dSlotFace, dClosure, dFB;
     DevBuf dOrdFlag, dOrdCnt, dOrdOff, dOrder, dOrdTotal;   // relaxation cell ordering
     DevBuf dPred, dHullOk, dTcErr;                          // surrogate predictions
@@ -671,12 +687,41 @@ struct SolverT : public fg_solver {
         return FG_OK;
     }
     int get_state(double *U, cudaStream_t s, bool wait) override {
+        const size_t ub = (size_t)nU * NV * sizeof(double);
+        if (wait) {
+            prof_begin(FG_K_OTHER, s);
+            launch_gather_state(nU, dU.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), s);
+            prof_end(s);
+            FG_LAUNCH_CHECK("get_state");
+            FG_CUDA_TRY(cudaMemcpyAsync(U, dStage.p, ub, cudaMemcpyDeviceToHost, s));
+            FG_CUDA_TRY(cudaStreamSynchronize(s));
+            return FG_OK;
+        }
+        if (!downStream) {
+            for (DevBuf &b : dStageOut) {
+                FG_CUDA_TRY(b.alloc(ub));
+                bytes += b.bytes;
+            }
+            FG_CUDA_TRY(cudaStreamCreateWithFlags(&downStream, cudaStreamNonBlocking));
+            for (cudaEvent_t &e : evOutFree) {
+                FG_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                FG_CUDA_TRY(cudaEventRecord(e, s));
+            }
+            FG_CUDA_TRY(cudaEventCreateWithFlags(&evGathered, cudaEventDisableTiming));
+        }
+        // the gather waits until the download two calls back has read this buffer; the copy
+        // overlaps whatever the caller queues on `s` next
+        const int b = outNext;
+        outNext ^= 1;
+        FG_CUDA_TRY(cudaStreamWaitEvent(s, evOutFree[b], 0));
         prof_begin(FG_K_OTHER, s);
-        launch_gather_state(nU, dU.as<double>(), dNew2Old.as<int32_t>(), dStage.as<double>(), s);
+        launch_gather_state(nU, dU.as<double>(), dNew2Old.as<int32_t>(), dStageOut[b].as<double>(), s);
         prof_end(s);
         FG_LAUNCH_CHECK("get_state");
-        FG_CUDA_TRY(cudaMemcpyAsync(U, dStage.p, (size_t)nU * NV * sizeof(double), cudaMemcpyDeviceToHost, s));
-        if (wait) FG_CUDA_TRY(cudaStreamSynchronize(s));
+        FG_CUDA_TRY(cudaEventRecord(evGathered, s));
+        FG_CUDA_TRY(cudaStreamWaitEvent(downStream, evGathered, 0));
+        FG_CUDA_TRY(cudaMemcpyAsync(U, dStageOut[b].p, ub, cudaMemcpyDeviceToHost, downStream));
+        FG_CUDA_TRY(cudaEventRecord(evOutFree[b], downStream));
         return FG_OK;
     }
     StageCoef coef(int irk, int writeU0) const {
@@ -1215,6 +1260,10 @@ int fg_get_state_async(fg_solver *s, double *U, void *stream) {
     FG_ENTER(s);
     if (!U) return set_err(FG_ERR_ARG, "fg_get_state_async: null U");
     return s->get_state(U, (cudaStream_t)stream, false);
+}
+int fg_state_join(fg_solver *s, void *stream) {
+    FG_ENTER(s);
+    return s->state_join((cudaStream_t)stream);
 }
 int fg_compute_rhs(fg_solver *s, int32_t want_signal, void *stream) {
     FG_ENTER(s);

@@ -275,9 +275,14 @@ int fg_set_state(fg_solver *s, const double *U, void *stream);
 int fg_set_state_async(fg_solver *s, const double *U, void *stream);
 /* Download U (nElem*10 doubles, reference order).  Synchronises `stream`. */
 int fg_get_state(fg_solver *s, double *U, void *stream);
-/* fg_get_state queued on `stream` without the synchronisation: U (pinned host memory for an
- * asynchronous copy) is complete once `stream` has passed the call. */
+/* fg_get_state without the synchronisation: the gather kernel is queued on `stream`, the copy
+ * into U (pinned host memory) on the solver's own download stream, so it overlaps the work the
+ * caller queues on `stream` next (two staging buffers: the third download in a row waits for
+ * the first to finish).  U is complete once a stream that waited through fg_state_join has passed
+ * that point, or after a device synchronisation. */
 int fg_get_state_async(fg_solver *s, double *U, void *stream);
+/* Make `stream` wait, on the device (no host wait), for every fg_get_state_async issued so far. */
+int fg_state_join(fg_solver *s, void *stream);
 
 /* ---------------------------------------------------------------- stage functions */
 

@@ -1,7 +1,8 @@
 """Asynchronous state transfer and the state probe through the C ABI.
 
 - fg_set_state_async + fg_step equals fg_set_state + fg_step bit for bit, and so does
-  fg_get_state_async after a stream synchronisation, over several back-to-back steps;
+  fg_get_state_async after fg_state_join and a stream synchronisation, over several back-to-back
+  steps; downloads queued back to back (more than the two staging buffers) each land intact;
 - a rejected asynchronous upload leaves the state as it was and is reported by fg_check_state
   and every fg_step until a good upload; the synchronous upload reports it at once;
 - fg_probe equals the oracle's conservation integral of variable 0 and numpy's extrema of the
@@ -35,8 +36,33 @@ def test_async_transfer_equals_sync(prec, meshdir):
         b.set_state_async(Uin.numpy(), stream=st.cuda_stream)
         b.step(stream=st.cuda_stream)
         b.get_state_async(Uout.numpy(), stream=st.cuda_stream)
+        b.state_join(stream=st.cuda_stream)
         st.synchronize()
         assert np.array_equal(Ua, Uout.numpy()), k
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_back_to_back_downloads(prec, meshdir):
+    m, c, U = make("tet_ref", meshdir, prec)
+    st = torch.cuda.Stream()
+    a = Solver(m, c, precision=prec)
+    b = Solver(m, c, precision=prec)
+    a.set_state(U)
+    b.set_state(U)
+    want, outs = [], []
+    for k in range(5):
+        a.step()
+        want.append(a.get_state())
+        b.step(stream=st.cuda_stream)
+        o = torch.empty(U.shape, dtype=torch.float64, pin_memory=True)
+        b.get_state_async(o.numpy(), stream=st.cuda_stream)
+        outs.append(o)
+    b.state_join(stream=st.cuda_stream)
+    st.synchronize()
+    for k in range(5):
+        assert np.array_equal(want[k], outs[k].numpy()), k
     a.close()
     b.close()
 
