@@ -72,6 +72,80 @@ __device__ __forceinline__ void rec_store(T *base, size_t stride, int c, const T
     }
 }
 
+// The gradient records G use the same component-major layout with vectors of 16 or 32 bytes per
+// precision: 32-byte vectors halve the vector loads of the face kernel (256-bit
+// ld.global.nc.v4.f64 / v8.f32).  FP64 records (36 values = 9 vectors of 4) take them: the FP64
+// face kernel measured 1-2 % faster; FP32 records would need padding to 40 values, and the FP32
+// face kernel measured 5 % slower with them.  grec_alloc<T>() values per cell are allocated.
+#ifndef FG_G_VEC_BYTES_F
+#define FG_G_VEC_BYTES_F 16
+#endif
+#ifndef FG_G_VEC_BYTES_D
+#define FG_G_VEC_BYTES_D 32
+#endif
+template <typename T>
+__host__ __device__ constexpr int gvec_bytes() { return sizeof(T) == 4 ? FG_G_VEC_BYTES_F : FG_G_VEC_BYTES_D; }
+template <typename T>
+__host__ __device__ constexpr int gvec() { return gvec_bytes<T>() / (int)sizeof(T); }
+template <typename T>
+__host__ __device__ constexpr int grec_alloc() { return (GREC + gvec<T>() - 1) / gvec<T>() * gvec<T>(); }
+template <typename T>
+__host__ __device__ inline size_t grec_index(size_t stride, size_t c, int v) {
+    return ((size_t)(v / gvec<T>()) * stride + c) * gvec<T>() + (size_t)(v % gvec<T>());
+}
+// one 32-byte vector: the loads read data that is not written during the kernel (non-coherent
+// path), the stores are ordinary
+__device__ __forceinline__ void ld32(const float *p, float *r) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
+        : "l"(p));
+}
+__device__ __forceinline__ void ld32(const double *p, double *r) {
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(r[0]), "=d"(r[1]), "=d"(r[2]), "=d"(r[3]) : "l"(p));
+}
+__device__ __forceinline__ void st32(float *p, const float *r) {
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(r[0]), "f"(r[1]), "f"(r[2]),
+                 "f"(r[3]), "f"(r[4]), "f"(r[5]), "f"(r[6]), "f"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void st32(double *p, const double *r) {
+    asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(r[0]), "d"(r[1]), "d"(r[2]), "d"(r[3])
+                 : "memory");
+}
+// the first NVAL values of the G record of cell c
+template <typename T, int NVAL>
+__device__ __forceinline__ void grec_load(const T *__restrict__ base, size_t stride, int c, T *out) {
+    if constexpr (gvec_bytes<T>() == 16) {
+        rec_load<T, NVAL>(base, stride, c, out);
+    } else {
+        constexpr int P = gvec<T>();
+#pragma unroll
+        for (int q = 0; q < (NVAL + P - 1) / P; q++) {
+            T x[P];
+            ld32(base + ((size_t)q * stride + c) * P, x);
+#pragma unroll
+            for (int j = 0; j < P; j++)
+                if (q * P + j < NVAL) out[q * P + j] = x[j];
+        }
+    }
+}
+// store NVAL values as the G record of cell c (the rest of the last vector is zero)
+template <typename T, int NVAL>
+__device__ __forceinline__ void grec_store(T *base, size_t stride, int c, const T *in) {
+    if constexpr (gvec_bytes<T>() == 16) {
+        rec_store<T, NVAL>(base, stride, c, in);
+    } else {
+        constexpr int P = gvec<T>();
+#pragma unroll
+        for (int q = 0; q < (NVAL + P - 1) / P; q++) {
+            T x[P];
+#pragma unroll
+            for (int j = 0; j < P; j++) x[j] = (q * P + j < NVAL) ? in[q * P + j] : (T)0;
+            st32(base + ((size_t)q * stride + c) * P, x);
+        }
+    }
+}
+
 template <typename T>
 struct PhysT {
     T gam[2], gm1[2], gp1[2], pinf[2], gpinf[2], cvgm1[2], gm1eta[2], mu[2];

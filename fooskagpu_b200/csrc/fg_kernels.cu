@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     for (int v = 0; v < NP; v++) out[v] = th[v];
 #pragma unroll
     for (int q = 0; q < NP * 3; q++) out[NP + q] = gs[q];
-    rec_store<T, GREC>(G, m.n, c, out);
+    grec_store<T, GREC>(G, m.n, c, out);
 }
 
 // MUSCL face state of a cell: w + theta * ((x_f - x_c) . grad w)  (DP/computeFaceValues.cu:66-105)
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(co
     {
         T g[GREC];
         rec_load<T, NP>(W, m.n, o, wo);
-        rec_load<T, GREC>(G, m.n, o, g);
+        grec_load<T, GREC>(G, m.n, o, g);
         face_state(wo, g, m.fdo[0][fi], m.fdo[1][fi], m.fdo[2][fi], sL);
 #pragma unroll
         for (int q = 0; q < 9; q++) gO[q] = g[NP + 9 + q];
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(co
     if (nb >= 0) {
         T wn[NP], g[GREC];
         rec_load<T, NP>(W, m.n, nb, wn);
-        rec_load<T, GREC>(G, m.n, nb, g);
+        grec_load<T, GREC>(G, m.n, nb, g);
         face_state(wn, g, m.fdn[0][fi], m.fdn[1][fi], m.fdn[2][fi], sR);
 #pragma unroll
         for (int q = 0; q < 9; q++) gN[q] = g[NP + 9 + q];
@@ -730,23 +730,23 @@ __global__ void k_copy(size_t cnt, const double *__restrict__ a, double *b) {
 // out[k * nval + v] = value v of the record of cells[k] (records of nRec cells, nval values each):
 // the records of the cells another part needs, packed whole
 template <typename T>
-__global__ void k_halo_pack(const T *__restrict__ rec, size_t nRec, int nval, const int32_t *__restrict__ cells,
+__global__ void k_halo_pack(const T *__restrict__ rec, size_t nRec, int nval, int vpv, const int32_t *__restrict__ cells,
                             int cnt, T *__restrict__ out) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)cnt * nval) return;
     const size_t k = i / nval;
     const int v = (int)(i - k * nval);
-    out[i] = rec[rec_index<T>(nRec, (size_t)cells[k], v)];
+    out[i] = rec[((size_t)(v / vpv) * nRec + (size_t)cells[k]) * vpv + (size_t)(v % vpv)];
 }
 // value v of the record of cells[k] = in[k * nval + v]: the ghosts' records received from their parts
 template <typename T>
-__global__ void k_halo_unpack(T *__restrict__ rec, size_t nRec, int nval, const int32_t *__restrict__ cells, int cnt,
-                              const T *__restrict__ in) {
+__global__ void k_halo_unpack(T *__restrict__ rec, size_t nRec, int nval, int vpv, const int32_t *__restrict__ cells,
+                              int cnt, const T *__restrict__ in) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)cnt * nval) return;
     const size_t k = i / nval;
     const int v = (int)(i - k * nval);
-    rec[rec_index<T>(nRec, (size_t)cells[k], v)] = in[i];
+    rec[((size_t)(v / vpv) * nRec + (size_t)cells[k]) * vpv + (size_t)(v % vpv)] = in[i];
 }
 
 // ------------------------------------------------------------------ launchers
@@ -805,19 +805,21 @@ void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, Stag
     k_update<T><<<(m.nU + 255) / 256, 256, 0, s>>>(m, f, D, sc);
 }
 template <typename T>
-void launch_halo_pack(const T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, T *out, cudaStream_t s) {
+void launch_halo_pack(const T *rec, size_t nRec, int nval, int vpv, const int32_t *cells, int cnt, T *out,
+                      cudaStream_t s) {
     const size_t tot = (size_t)cnt * nval;
-    if (tot) k_halo_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, nRec, nval, cells, cnt, out);
+    if (tot) k_halo_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, nRec, nval, vpv, cells, cnt, out);
 }
 template <typename T>
-void launch_halo_unpack(T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, const T *in, cudaStream_t s) {
+void launch_halo_unpack(T *rec, size_t nRec, int nval, int vpv, const int32_t *cells, int cnt, const T *in,
+                        cudaStream_t s) {
     const size_t tot = (size_t)cnt * nval;
-    if (tot) k_halo_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, nRec, nval, cells, cnt, in);
+    if (tot) k_halo_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rec, nRec, nval, vpv, cells, cnt, in);
 }
-template void launch_halo_pack<float>(const float *, size_t, int, const int32_t *, int, float *, cudaStream_t);
-template void launch_halo_pack<double>(const double *, size_t, int, const int32_t *, int, double *, cudaStream_t);
-template void launch_halo_unpack<float>(float *, size_t, int, const int32_t *, int, const float *, cudaStream_t);
-template void launch_halo_unpack<double>(double *, size_t, int, const int32_t *, int, const double *, cudaStream_t);
+template void launch_halo_pack<float>(const float *, size_t, int, int, const int32_t *, int, float *, cudaStream_t);
+template void launch_halo_pack<double>(const double *, size_t, int, int, const int32_t *, int, double *, cudaStream_t);
+template void launch_halo_unpack<float>(float *, size_t, int, int, const int32_t *, int, const float *, cudaStream_t);
+template void launch_halo_unpack<double>(double *, size_t, int, int, const int32_t *, int, const double *, cudaStream_t);
 template <typename T>
 void launch_prim(int n, const double *U, T *W, size_t wStride, const PhysD &D, cudaStream_t s) {
     k_prim<T><<<(n + 255) / 256, 256, 0, s>>>(n, U, W, wStride, D);

@@ -115,7 +115,8 @@ struct Fields {
     double *RHS;        // [10][n] (RHS-mode residual)
     T *Win;             // primitive records (WREC values per cell, component-major) read this stage
     T *Wout;            // primitive records written this stage
-    T *G;               // limiter + gradient records (GREC values per cell, component-major)
+    T *G;               // limiter + gradient records (GREC values per cell, component-major vectors of
+                        // gvec_bytes<T>() bytes, grec_alloc<T>() values per cell allocated)
     double *signal;     // [n]
     T *cellSig;         // [n] per-cell maximum face signal speed of a dt step (zeroed before it)
     double *blockMin;   // [nBlocks]
@@ -160,12 +161,14 @@ void launch_update(const DevMesh<T> &m, const Fields<T> &f, const PhysD &D, Stag
 // primitive records of the first n cells from U (records of wStride cells)
 template <typename T>
 void launch_prim(int n, const double *U, T *W, size_t wStride, const PhysD &D, cudaStream_t s);
-// partitioned runs: the records (nval values each, records of nRec cells) of cells[0..cnt) to /
-// from a contiguous buffer of whole records
+// partitioned runs: the records (nval values each, records of nRec cells in vectors of vpv
+// values) of cells[0..cnt) to / from a contiguous buffer of whole records
 template <typename T>
-void launch_halo_pack(const T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, T *out, cudaStream_t s);
+void launch_halo_pack(const T *rec, size_t nRec, int nval, int vpv, const int32_t *cells, int cnt, T *out,
+                      cudaStream_t s);
 template <typename T>
-void launch_halo_unpack(T *rec, size_t nRec, int nval, const int32_t *cells, int cnt, const T *in, cudaStream_t s);
+void launch_halo_unpack(T *rec, size_t nRec, int nval, int vpv, const int32_t *cells, int cnt, const T *in,
+                        cudaStream_t s);
 // dt steps of the fused path: per cell (own cells, blocks of the gather kernel) the CFL bound
 // volP / cellSig and the signal, the block minima into blockMin[flux_blocks(nU)]
 template <typename T>

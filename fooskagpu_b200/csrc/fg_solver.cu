@@ -253,7 +253,7 @@ __global__ void k_field_vars(int n, const double *__restrict__ U, const T *__res
     const double tG = (pG + D.pinf[1]) / ((cp[1] / D.gam[1]) * D.gm1[1] * rG);
     // grad rho = (rhoL - rhoG) grad alpha + alpha grad rhoL + (1 - alpha) grad rhoG
     // gradients of W: component d of var v is value NP + 3 v + d of the record
-    auto g = [&](int q) { return (double)G[rec_index<T>(gStride, (size_t)c, NP + q)]; };
+    auto g = [&](int q) { return (double)G[grec_index<T>(gStride, (size_t)c, NP + q)]; };
     double gr[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) gr[d] = (rL - rG) * g(d) + aL * g(3 + d) + aG * g(6 + d);
@@ -567,7 +567,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(dStage.alloc(u));
         FG_CUDA_TRY(dW[0].alloc((size_t)n * WREC * sizeof(T)));
         FG_CUDA_TRY(dW[1].alloc((size_t)n * WREC * sizeof(T)));
-        FG_CUDA_TRY(dG.alloc((size_t)n * GREC * sizeof(T)));
+        FG_CUDA_TRY(dG.alloc((size_t)n * grec_alloc<T>() * sizeof(T)));
         FG_CUDA_TRY(dSig.alloc((size_t)n * sizeof(double)));
         FG_CUDA_TRY(dCellSig.alloc((size_t)n * sizeof(T)));
         FG_CUDA_TRY(dBlockMin.alloc((size_t)std::max(flux_blocks(n), cons_blocks(n)) * sizeof(double)));
@@ -588,7 +588,7 @@ struct SolverT : public fg_solver {
         FG_CUDA_TRY(cudaMemset(dRHS.p, 0, u));
         FG_CUDA_TRY(cudaMemset(dW[0].p, 0, (size_t)n * WREC * sizeof(T)));
         FG_CUDA_TRY(cudaMemset(dW[1].p, 0, (size_t)n * WREC * sizeof(T)));
-        FG_CUDA_TRY(cudaMemset(dG.p, 0, (size_t)n * GREC * sizeof(T)));
+        FG_CUDA_TRY(cudaMemset(dG.p, 0, (size_t)n * grec_alloc<T>() * sizeof(T)));
         const double scal[4] = {cs.dt, 0.0, 0.0, 0.0};
         FG_CUDA_TRY(cudaMemcpy(dScal.p, scal, sizeof(scal), cudaMemcpyHostToDevice));
         bytes = 0;
@@ -757,16 +757,18 @@ struct SolverT : public fg_solver {
             return set_err(FG_ERR_ARG, "partitioned mesh: set the transport with fg_solver_set_halo first");
         T *rec = (field == FG_HALO_W) ? dW[cur].as<T>() : dG.as<T>();
         const int stride = (field == FG_HALO_W) ? WREC : GREC;
+        const int vpvRec = (field == FG_HALO_W) ? vpv<T>() : gvec<T>();
         const int nSend = sendStart.back(), nRecv = recvStart.back();
         prof_begin(FG_K_OTHER, s);
-        launch_halo_pack<T>(rec, (size_t)n, stride, dSendCells.as<int32_t>(), nSend, static_cast<T *>(haloSend), s);
+        launch_halo_pack<T>(rec, (size_t)n, stride, vpvRec, dSendCells.as<int32_t>(), nSend, static_cast<T *>(haloSend), s);
         prof_end(s);
         FG_LAUNCH_CHECK("halo pack");
         FG_CUDA_TRY(cudaStreamSynchronize(s));
         if (halo.exchange(halo.ctx, field, (int64_t)stride * (int64_t)sizeof(T), s) != 0)
             return set_err(FG_ERR_CUDA, "partitioned run: halo exchange failed");
         prof_begin(FG_K_OTHER, s);
-        launch_halo_unpack<T>(rec, (size_t)n, stride, dRecvCells.as<int32_t>(), nRecv, static_cast<const T *>(haloRecv), s);
+        launch_halo_unpack<T>(rec, (size_t)n, stride, vpvRec, dRecvCells.as<int32_t>(), nRecv,
+                            static_cast<const T *>(haloRecv), s);
         prof_end(s);
         FG_LAUNCH_CHECK("halo unpack");
         return FG_OK;
@@ -971,16 +973,16 @@ struct SolverT : public fg_solver {
     }
     int get_limited(double *grad, double *theta) override {
         FG_CUDA_TRY(cudaDeviceSynchronize());
-        std::vector<T> g((size_t)n * GREC);
+        std::vector<T> g((size_t)n * grec_alloc<T>());
         std::vector<int32_t> n2o(nU);
         FG_CUDA_TRY(cudaMemcpy(g.data(), dG.p, g.size() * sizeof(T), cudaMemcpyDeviceToHost));
         FG_CUDA_TRY(cudaMemcpy(n2o.data(), dNew2Old.p, (size_t)nU * sizeof(int32_t), cudaMemcpyDeviceToHost));
         for (int i = 0; i < nU; i++) {
             const size_t o = (size_t)n2o[i];
             for (int v = 0; v < NV; v++) {
-                if (theta) theta[o * NV + v] = (v < NP) ? (double)g[rec_index<T>((size_t)n, i, v)] : 0.0;
+                if (theta) theta[o * NV + v] = (v < NP) ? (double)g[grec_index<T>((size_t)n, i, v)] : 0.0;
                 for (int d = 0; d < 3; d++)
-                    if (grad) grad[(o * NV + v) * 3 + d] = (v < NP) ? (double)g[rec_index<T>((size_t)n, i, NP + 3 * v + d)] : 0.0;
+                    if (grad) grad[(o * NV + v) * 3 + d] = (v < NP) ? (double)g[grec_index<T>((size_t)n, i, NP + 3 * v + d)] : 0.0;
             }
         }
         return FG_OK;
