@@ -43,7 +43,7 @@ class FgCase(C.Structure):
         ("dynVisc", f64 * 2), ("heatCoef", f64 * 2), ("Pr", f64 * 2),
         ("relaxFlag", i32), ("hllcEnergyFix", i32), ("hllcTieTol", f64), ("heatFlux", i32),
         ("limiter", i32), ("inletVelFlag", i32), ("inletStateFlag", i32), ("reserved", i32 * 2),
-        ("inletVel", f64 * 3), ("inletP", f64), ("inletT", f64),
+        ("inletVel", f64 * 3), ("inletP", f64), ("inletT", f64), ("pressureDatum", f64),
     ]
 
 

@@ -195,7 +195,7 @@ def water_vapour_constants(gamma_l=6.12, pinf_l=3.43e8, gamma_v=1.33, pinf_v=0.0
     return dict(gamma=(gamma_l, gamma_v), pInf=(pinf_l, pinf_v), Cp=(cpl, cpv), eta=(etal, etav), satConst=(0.0, qv))
 
 
-def water_vapour_case(rk=3, cfl=0.5, adapt_itr=10, limiter=1, viscous=True, base=None) -> FgCase:
+def water_vapour_case(rk=3, cfl=0.5, adapt_itr=10, limiter=1, viscous=True, base=None, p_datum=1e7) -> FgCase:
     """Water / vapour homogeneous mixture with Gibbs-equilibrium mass transfer (per-cell Newton),
     HLLC + MUSCL with the van Albada-type limiter (limiter = 1), SSP-RK3; laminar viscosity of
     water (1.0e-3 Pa s) and vapour (9.7e-6 Pa s) at 20 C, no turbulence model.  The wave speeds
@@ -203,9 +203,13 @@ def water_vapour_case(rk=3, cfl=0.5, adapt_itr=10, limiter=1, viscous=True, base
     water / vapour mixture is a few m/s, and with it as the HLLC wave-speed estimate and in the
     CFL bound the reference scheme blows up in the first steps of the bubble collapse.  The
     other INPUT fields keep the reference's values (DP/buildInput.cu:10-69); dt adapts every
-    adapt_itr steps."""
+    adapt_itr steps.  The pressure datum (fg_case.pressureDatum) is p_datum, the ambient pressure
+    (10 MPa for the bubble's liquid): the reduced-precision face momentum flux then carries no
+    rounding of the ambient pressure, whose spurious velocities would make the reference's
+    absolute-tolerance thermal Newton iterate on the stiff minor phase (0 = the reference's form)."""
     c = _start(base)
     c.woodsFlag = 0
+    c.pressureDatum = p_datum
     k = water_vapour_constants()
     for m in range(2):
         c.gamma[m] = k["gamma"][m]
@@ -272,7 +276,7 @@ def jet_case(u_jet=200.0, p_gas=5e6, T=298.15, rk=3, cfl=0.3, base=None) -> FgCa
     (0, 0, u_jet) and the inlet state (p_gas, T) instead of the reference's fixed one.  The time
     step adapts every step at CFL 0.3: the CFL bound sees the gas until the liquid (four times
     the sound speed) has entered a cell, and a dt held over ten steps blows up at the inlet."""
-    c = water_vapour_case(rk=rk, cfl=cfl, adapt_itr=1, limiter=0, viscous=True, base=base)
+    c = water_vapour_case(rk=rk, cfl=cfl, adapt_itr=1, limiter=0, viscous=True, base=base, p_datum=p_gas)
     c.turbulence = 1
     c.inletVelFlag = 1
     c.inletVel[0], c.inletVel[1], c.inletVel[2] = 0.0, 0.0, u_jet

@@ -155,12 +155,14 @@ struct PhysT {
     T tieTol;      // |S*| <= tieTol (|S_L| + |S_R|) counts as S* = 0 (extension; 0 = reference)
     T cp[2], prn[2];   // heat conduction (extension): k = cp mu / Pr
     T inVel[3];        // prescribed inlet velocity (extension, inVelFlag)
+    T pDatum;          // pressure datum of the face momentum flux (extension, 0 = reference)
     int woods, visc, turb, energyFix, heat, limiter, inVelFlag;
 };
 
 struct PhysD {
     double gam[2], gm1[2], pinf[2], gpinf[2], cvgm1[2], gm1eta[2];
     double avfLo, avfHi;
+    double pDatum;     // pressure datum of the cell-centre pressure term (PhysT::pDatum)
 };
 
 // ---------------------------------------------------------------- equation of state

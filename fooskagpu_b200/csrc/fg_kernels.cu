@@ -295,9 +295,12 @@ __device__ __forceinline__ T face_tail(const PhysT<T> &P, const T *sL, const T *
     T H[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) H[v] = A * F[v];
-    H[3] += A * pF * nx;
-    H[4] += A * pF * ny;
-    H[5] += A * pF * nz;
+    // the face pressure relative to the datum P0; the gather adds (p_C - P0) times the cell's
+    // sum of outward n A, so the residual is the same for every P0 in exact arithmetic
+    const T pd = pF - P.pDatum;
+    H[3] += A * pd * nx;
+    H[4] += A * pd * ny;
+    H[5] += A * pd * nz;
     if (P.visc) {
         T gv[9];
 #pragma unroll
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(FG_GATHER_THREADS, MinBlocks<T>::gather) k_gat
         T w[NP];
         rec_load<T, NP>(f.Win, m.n, c, w);
         const double a = w[0], pl = w[6], pg = w[7];
-        const double pc = (double)(w[0] * w[6] + (1 - w[0]) * w[7]);
+        const double pc = (double)(w[0] * w[6] + (1 - w[0]) * w[7]) - D.pDatum;
         acc[0] -= a * su;
         acc[6] += a * pl * su;
         acc[7] += (1.0 - a) * pg * su;

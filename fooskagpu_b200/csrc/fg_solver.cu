@@ -349,6 +349,8 @@ struct SolverT : public fg_solver {
         P.limiter = cs.limiter;
         P.inVelFlag = (cs.inletVelFlag == 1);
         for (int d = 0; d < 3; d++) P.inVel[d] = (T)cs.inletVel[d];
+        P.pDatum = (T)cs.pressureDatum;
+        D.pDatum = (double)P.pDatum;   // the face and cell terms use the same datum value
         if (cs.limiter != 0 && cs.limiter != 1) return set_err(FG_ERR_UNSUPPORTED, "limiter must be 0 or 1");
         if (P.heat && !(cs.Pr[0] > 0 && cs.Pr[1] > 0))
             return set_err(FG_ERR_ARG, "heatFlux needs Pr[0] > 0 and Pr[1] > 0");

@@ -125,6 +125,12 @@ typedef struct fg_case {
     double  inletVel[3];
     double  inletP;
     double  inletT;
+    /* pressureDatum (Pa, 0 = the reference's form): the face momentum flux carries A (p_F - P0) n
+     * and the cell-centre pressure term (p_C - P0) times the cell's sum of outward n A, the same
+     * residual in exact arithmetic.  With P0 near the ambient pressure the reduced-precision face
+     * math carries no rounding of the ambient pressure into the momentum residual (at rest:
+     * none at all), where it would otherwise raise spurious velocities of order eps p / (rho c). */
+    double  pressureDatum;
 } fg_case;
 
 /* Fill *c with the values the reference hard-codes in DP/buildInput.cu:10-69. */
