@@ -18,7 +18,7 @@ EXE = HERE / "_ref" / "fooska_ref_dp"
 
 # case fields of ours that the reference's INPUT struct does not have
 EXTENSION_KEYS = ("relaxFlag", "hllcEnergyFix", "hllcTieTol", "heatFlux", "limiter", "inletVelFlag", "reserved",
-                  "inletVel", "inletStateFlag", "inletP", "inletT")
+                  "inletVel", "inletStateFlag", "inletP", "inletT", "pressureDatum")
 
 
 def available() -> bool:
