@@ -459,7 +459,8 @@ int fg_launch_count(fg_solver *s, uint64_t *count);
  *   fg_get_limited: grad[nElem*10*3] and theta[nElem*10] of the last residual (vars 0..8;
  *                   var 9, the mixture density the reference also limits but never uses,
  *                   is returned as 0)
- *   fg_get_signal: per-cell max signal speed of the last fg_compute_rhs(want_signal=1) */
+ *   fg_get_signal: per-cell max signal speed of the last fg_compute_rhs(want_signal=1) or of the
+ *                   last dt step of fg_step (which computes it in the face kernel instead) */
 int fg_get_rhs(fg_solver *s, double *rhs);
 int fg_get_limited(fg_solver *s, double *grad, double *theta);
 int fg_get_signal(fg_solver *s, double *signal);
