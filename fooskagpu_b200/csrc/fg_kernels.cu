@@ -146,6 +146,17 @@ __device__ __forceinline__ T limiter_phi(T num, T diff) {
     return num / (2 * diff);
 }
 
+// slot loops of the gradient kernel: unrolled to the largest face count (the loads of every slot
+// can then be issued early), or a plain loop to the cell's face count
+#ifndef FG_GRAD_UNROLL
+#define FG_GRAD_UNROLL 1
+#endif
+#if FG_GRAD_UNROLL
+#define FG_GRAD_SLOT_LOOP(k, nf) _Pragma("unroll") for (int k = 0; k < MAXSLOT; k++) if (k < (nf))
+#else
+#define FG_GRAD_SLOT_LOOP(k, nf) for (int k = 0; k < (nf); k++)
+#endif
+
 // kLim: 0 the reference's limiter function, 1 the van Albada-type extension (fg_case.limiter)
 template <typename T, int kLim>
 __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_grad(const DevMesh<T> m, const T *__restrict__ W,
@@ -197,7 +208,7 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     }
     const int fl = m.flags[c];
     const int nf = fl & 7;
-    for (int k = 0; k < nf; k++) {
+    FG_GRAD_SLOT_LOOP(k, nf) {
         const int li = geo.local(k);
         // outward n A of the face (the host computed (+-1) n A in T arithmetic, as the reference's
         // sign times normal times area)
@@ -235,7 +246,7 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     T dpos[NP], dneg[NP];
 #pragma unroll
     for (int v = 0; v < NP; v++) dpos[v] = dneg[v] = 0;
-    for (int k = 0; k < nf; k++) {
+    FG_GRAD_SLOT_LOOP(k, nf) {
         const T dx = geo.get(3, k), dy = geo.get(4, k), dz = geo.get(5, k);
 #pragma unroll
         for (int v = 0; v < NP; v++) {
