@@ -80,7 +80,8 @@ class FgRelaxStats(C.Structure):
 
 
 class FgPartitionInfo(C.Structure):
-    _fields_ = [("nParts", i32), ("part", i32), ("nOwned", i32), ("nGhost", i32), ("nSend", i32), ("nRecv", i32)]
+    _fields_ = [("nParts", i32), ("part", i32), ("nOwned", i32), ("nGhost", i32), ("nSend", i32), ("nRecv", i32),
+                ("nGhost1", i32)]
 
 
 FG_HALO_W, FG_HALO_G = 0, 1

@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(StageCells<T>::value, MinBlocks<T>::grad) k_gr
     const int b = blockIdx.x;
     const int B = m.blockCells;
     const int lo = b * B;
-    const int nOwn = min(B, m.nU - lo);      // cells whose gradients this block computes
+    const int nOwn = min(B, m.nG - lo);      // cells whose gradients this block computes
     const int nBlockRecs = min(B, m.n - lo);  // cells of the block range with records (ghosts of a part too)
     const int nRec = B + (m.haloStart[b + 1] - m.haloStart[b]);
     const int SS = slot_stride(m.nSlots);
@@ -376,7 +376,7 @@ template <typename T>
 __global__ void __launch_bounds__(FG_FACE_THREADS, MinBlocks<T>::face) k_face(const DevMesh<T> m, const T *__restrict__ W, const T *__restrict__ G,
                                               T *__restrict__ FB, T *cellSig, const PhysT<T> P, int wantSignal) {
     const int fi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (fi >= m.nF) return;
+    if (fi >= m.nFEval) return;
     const int o = m.fOwn[fi];
     const int nb = m.fNb[fi];
     const T nx = m.fnx[fi], ny = m.fny[fi], nz = m.fnz[fi], A = m.fA[fi];
@@ -792,7 +792,7 @@ int stage_kernels_setup(const DevMesh<T> &m) {
 }
 template <typename T>
 void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cudaStream_t s) {
-    const int nb = (m.nU + m.blockCells - 1) / m.blockCells;
+    const int nb = (m.nG + m.blockCells - 1) / m.blockCells;
     if (P.limiter == 1)
         k_grad<T, 1><<<nb, m.blockCells, grad_smem(m), s>>>(m, f.Win, f.G, P);
     else
@@ -800,7 +800,8 @@ void launch_grad(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, cud
 }
 template <typename T>
 void launch_face(const DevMesh<T> &m, const Fields<T> &f, const PhysT<T> &P, int wantSignal, cudaStream_t s) {
-    k_face<T><<<(m.nF + FG_FACE_THREADS - 1) / FG_FACE_THREADS, FG_FACE_THREADS, 0, s>>>(m, f.Win, f.G, f.FB, f.cellSig, P,
+    if (m.nFEval == 0) return;
+    k_face<T><<<(m.nFEval + FG_FACE_THREADS - 1) / FG_FACE_THREADS, FG_FACE_THREADS, 0, s>>>(m, f.Win, f.G, f.FB, f.cellSig, P,
                                                                                       wantSignal);
 }
 template <typename T>

@@ -10,6 +10,8 @@ template <typename T>
 struct DevMesh {
     int n;              // cells with records (W, G): own cells, then the ghosts of a partitioned mesh
     int nU;             // own cells: the first nU cells carry a state (U, U0, RHS rows) and are updated
+    int nG;             // cells with gradients: own cells, then a part's first-layer ghosts
+    int nFEval;         // faces the face kernel evaluates (those touching an own cell) come first
     int nSlots;         // max faces per cell
     const int32_t *nbr;   // neighbour cell, or -bc (1..5) on a boundary slot, or INT32_MIN unused
     const int32_t *flags; // bits 0-2: faces of the cell; bit 3+k: cell owns the face of slot k

@@ -40,15 +40,21 @@ struct Mesh {
     // ---- device ordering ----
     std::vector<int32_t> new2old, old2new;
     // ---- part of a partitioned mesh (partition_mesh): cells [0, nOwned) are the part's own,
-    // cells [nOwned, nElem) its ghosts (face neighbours owned by other parts) ----
+    // cells [nOwned, nOwned + nGhost1) its first ghost layer (face neighbours owned by other
+    // parts: the part computes their gradients, so the mesh holds all their faces), cells
+    // [nOwned + nGhost1, nElem) the second layer (their other neighbours: records only) ----
     int nOwned = -1;                       // -1: not partitioned, every cell owned
+    int nGhost1 = 0;
     int nParts = 1, part = 0;
     std::vector<int32_t> cellGlobal;       // reference (.neu) index in the whole mesh of each cell
     // cells whose records go to / come from each part q: sendCells[sendStart[q] .. sendStart[q+1])
-    // (own cells), recvCells[recvStart[q] .. recvStart[q+1]) (ghosts), both in the whole mesh's
-    // device order, so that the k-th record part p sends to q is q's k-th ghost from p
+    // (own cells within two face hops of q's), recvCells[recvStart[q] .. recvStart[q+1]) (ghosts
+    // of both layers owned by q), both in the whole mesh's device order, so that the k-th record
+    // part p sends to q is q's k-th ghost from p
     std::vector<int32_t> sendStart, sendCells, recvStart, recvCells;
     int owned() const { return nOwned < 0 ? nElem : nOwned; }
+    // cells whose gradients the part computes: own and first-layer ghosts
+    int gradient_cells() const { return nOwned < 0 ? nElem : nOwned + nGhost1; }
 };
 
 // Parse a Gambit neutral file with the reference's grammar (DP/translator.cu:3-354).

@@ -3,12 +3,14 @@
 // Replaces the reference's METIS decomposition and local-mesh build (DP/decompose.cu:52,
 // DP/buildLocalMesh.cu): part p owns the cells of the contiguous range
 // [floor(n p / P), floor(n (p+1) / P)) of the mesh's device order (Morton order of the cell
-// centres, so a part is a compact region), plus one layer of ghost cells, its face neighbours in
-// other parts.  The local mesh keeps every face that touches an own cell with the whole mesh's
-// orientation (owner, neighbour), geometry and boundary code, so each face flux and each cell
-// update is computed from the same numbers as in the unpartitioned run.  Per stage the parts
-// exchange the primitive records and then the gradient records of the halo cells (the
-// reference's communicate step, DP/communicate.cu), through the caller's transport.
+// centres, so a part is a compact region), plus two layers of ghost cells: the first layer, face
+// neighbours of own cells in other parts, and the second, their face neighbours in neither.  The
+// local mesh keeps every face that touches an own or a first-layer cell with the whole mesh's
+// orientation (owner, neighbour), geometry and boundary code, so a part computes the gradients of
+// its first-layer ghosts itself, from the same numbers as their owner, and each face flux and each
+// cell update from the same numbers as in the unpartitioned run.  Per stage the parts exchange
+// only the primitive records of the ghosts (the reference's communicate step, DP/communicate.cu,
+// exchanges values and gradients), through the caller's transport.
 #include "fg_mesh.h"
 
 #include <algorithm>
@@ -37,25 +39,40 @@ int partition_mesh(const Mesh &g, int P, int p, Mesh &l, std::string &err) {
     };
     const int lo = first(p), hi = first(p + 1);
     const int nOwn = hi - lo;
-    // faces touching an own cell (whole-mesh face order) and the ghosts they reach
-    std::vector<int32_t> faces, ghosts;
+    auto own = [&](int j) { return j >= lo && j < hi; };
+    auto dev = [&](int f, int side) { return g.old2new[g.fc2el[2 * f + side]]; };
+    // layer 1: the other parts' face neighbours of own cells
+    std::vector<uint8_t> layer(n, 0);   // 1 own, 2 first ghost layer, 3 second
+    for (int j = lo; j < hi; j++) layer[j] = 1;
+    std::vector<int32_t> ghosts1, ghosts2;
     for (int f = 0; f < g.nFcs; f++) {
-        const int a = g.old2new[g.fc2el[2 * f]];
+        if (g.boundCond[f] != 0) continue;
+        const int a = dev(f, 0), b = dev(f, 1);
+        if (own(a) && !own(b) && !layer[b]) { layer[b] = 2; ghosts1.push_back(b); }
+        if (own(b) && !own(a) && !layer[a]) { layer[a] = 2; ghosts1.push_back(a); }
+    }
+    // layer 2 and the faces: every face touching an own or a first-layer cell
+    std::vector<int32_t> faces;
+    for (int f = 0; f < g.nFcs; f++) {
         const bool interior = g.boundCond[f] == 0;
-        const int b = interior ? g.old2new[g.fc2el[2 * f + 1]] : -1;
-        const bool inA = a >= lo && a < hi, inB = interior && b >= lo && b < hi;
+        const int a = dev(f, 0), b = interior ? dev(f, 1) : -1;
+        const bool inA = layer[a] == 1 || layer[a] == 2, inB = interior && (layer[b] == 1 || layer[b] == 2);
         if (!inA && !inB) continue;
         faces.push_back(f);
-        if (interior && !inA) ghosts.push_back(a);
-        if (interior && !inB) ghosts.push_back(b);
+        if (interior && !layer[a]) { layer[a] = 3; ghosts2.push_back(a); }
+        if (interior && !layer[b]) { layer[b] = 3; ghosts2.push_back(b); }
     }
-    std::sort(ghosts.begin(), ghosts.end());
-    ghosts.erase(std::unique(ghosts.begin(), ghosts.end()), ghosts.end());
-    const int nL = nOwn + (int)ghosts.size();
-    // device index of the whole mesh -> local cell
-    std::vector<int32_t> localOf(n, -1);
+    std::sort(ghosts1.begin(), ghosts1.end());
+    std::sort(ghosts2.begin(), ghosts2.end());
+    const int n1 = (int)ghosts1.size();
+    const int nL = nOwn + n1 + (int)ghosts2.size();
+    // device index of the whole mesh -> local cell: own, then the first layer, then the second
+    std::vector<int32_t> localOf(n, -1), globalOf(nL);
     for (int j = lo; j < hi; j++) localOf[j] = j - lo;
-    for (size_t k = 0; k < ghosts.size(); k++) localOf[ghosts[k]] = nOwn + (int)k;
+    for (int k = 0; k < n1; k++) localOf[ghosts1[k]] = nOwn + k;
+    for (size_t k = 0; k < ghosts2.size(); k++) localOf[ghosts2[k]] = nOwn + n1 + (int)k;
+    for (int j = 0; j < n; j++)
+        if (localOf[j] >= 0) globalOf[localOf[j]] = j;
 
     l = Mesh();
     l.nElem = nL;
@@ -68,7 +85,7 @@ int partition_mesh(const Mesh &g, int P, int p, Mesh &l, std::string &err) {
     l.elFcCenter.resize((size_t)nL * 18);
     l.volume.resize(nL);
     for (int c = 0; c < nL; c++) {
-        const int j = c < nOwn ? lo + c : ghosts[c - nOwn];
+        const int j = globalOf[c];
         const int e = g.new2old[j];
         l.cellGlobal[c] = e;
         l.elNN[c] = g.elNN[e];
@@ -98,8 +115,8 @@ int partition_mesh(const Mesh &g, int P, int p, Mesh &l, std::string &err) {
     for (int i = 0; i < nF; i++) {
         const int f = faces[i];
         const bool interior = g.boundCond[f] == 0;
-        l.fc2el[2 * i] = localOf[g.old2new[g.fc2el[2 * f]]];
-        l.fc2el[2 * i + 1] = interior ? localOf[g.old2new[g.fc2el[2 * f + 1]]] : g.fc2el[2 * f + 1];
+        l.fc2el[2 * i] = localOf[dev(f, 0)];
+        l.fc2el[2 * i + 1] = interior ? localOf[dev(f, 1)] : g.fc2el[2 * f + 1];
         l.fc2elFc[2 * i] = g.fc2elFc[2 * f];
         l.fc2elFc[2 * i + 1] = g.fc2elFc[2 * f + 1];
         l.boundCond[i] = g.boundCond[f];
@@ -121,23 +138,52 @@ int partition_mesh(const Mesh &g, int P, int p, Mesh &l, std::string &err) {
     l.new2old.resize(nL);
     l.old2new.resize(nL);
     for (int c = 0; c < nL; c++) l.new2old[c] = l.old2new[c] = c;
-    // halo lists: ghosts grouped by owning part (ghosts are sorted by device index and the parts
-    // are contiguous ranges of it, so the groups are contiguous); own cells sent to each part
+    // halo lists.  A part needs the records of every cell within two face hops of its own cells
+    // (its two ghost layers); received grouped by owning part, each group in device order
+    std::vector<int32_t> ghostsAll(ghosts1);
+    ghostsAll.insert(ghostsAll.end(), ghosts2.begin(), ghosts2.end());
+    std::sort(ghostsAll.begin(), ghostsAll.end());
     l.recvStart.assign(P + 1, 0);
-    for (int gi : ghosts) l.recvStart[part_of(gi) + 1]++;
+    for (int gi : ghostsAll) l.recvStart[part_of(gi) + 1]++;
     for (int q = 0; q < P; q++) l.recvStart[q + 1] += l.recvStart[q];
-    l.recvCells.resize(ghosts.size());
-    for (size_t k = 0; k < ghosts.size(); k++) l.recvCells[k] = nOwn + (int)k;
-    std::vector<int64_t> pairs;   // (part, own local cell)
+    l.recvCells.resize(ghostsAll.size());
+    for (size_t k = 0; k < ghostsAll.size(); k++) l.recvCells[k] = localOf[ghostsAll[k]];
+    // an own cell goes to every other part with a cell within two face hops of it (it is in that
+    // part's ghost layers); the local mesh holds every face of its own and first-layer cells
+    std::vector<int32_t> adjStart(nL + 1, 0), adj;
     for (int i = 0; i < nF; i++) {
-        const int a = l.fc2el[2 * i];
         if (l.boundCond[i] != 0) continue;
-        const int b = l.fc2el[2 * i + 1];
-        if (a < nOwn && b >= nOwn) pairs.push_back((int64_t)part_of(ghosts[b - nOwn]) * nL + a);
-        if (b < nOwn && a >= nOwn) pairs.push_back((int64_t)part_of(ghosts[a - nOwn]) * nL + b);
+        adjStart[l.fc2el[2 * i] + 1]++;
+        adjStart[l.fc2el[2 * i + 1] + 1]++;
+    }
+    for (int c = 0; c < nL; c++) adjStart[c + 1] += adjStart[c];
+    adj.resize(adjStart[nL]);
+    {
+        std::vector<int32_t> fill(adjStart.begin(), adjStart.end() - 1);
+        for (int i = 0; i < nF; i++) {
+            if (l.boundCond[i] != 0) continue;
+            const int a = l.fc2el[2 * i], b = l.fc2el[2 * i + 1];
+            adj[fill[a]++] = b;
+            adj[fill[b]++] = a;
+        }
+    }
+    std::vector<int64_t> pairs;   // (part, own local cell)
+    std::vector<int32_t> seen(P, -1);
+    for (int c = 0; c < nOwn; c++) {
+        auto mark = [&](int x) {
+            const int q = part_of(globalOf[x]);
+            if (q != p && seen[q] != c) {
+                seen[q] = c;
+                pairs.push_back((int64_t)q * nL + c);
+            }
+        };
+        for (int k = adjStart[c]; k < adjStart[c + 1]; k++) {
+            const int d = adj[k];
+            mark(d);
+            for (int k2 = adjStart[d]; k2 < adjStart[d + 1]; k2++) mark(adj[k2]);
+        }
     }
     std::sort(pairs.begin(), pairs.end());
-    pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
     l.sendStart.assign(P + 1, 0);
     l.sendCells.resize(pairs.size());
     for (size_t k = 0; k < pairs.size(); k++) {
@@ -146,6 +192,7 @@ int partition_mesh(const Mesh &g, int P, int p, Mesh &l, std::string &err) {
     }
     for (int q = 0; q < P; q++) l.sendStart[q + 1] += l.sendStart[q];
     l.nOwned = nOwn;
+    l.nGhost1 = n1;
     l.nParts = P;
     l.part = p;
     return FG_OK;

@@ -171,6 +171,8 @@ struct fg_solver {
     long long logCap = 0;
     int n = 0, nSlots = 0;
     int nU = 0;               // own cells: the state rows (n - nU ghosts on a partitioned mesh)
+    int nG = 0;               // cells with gradients: own and first-layer ghost cells
+    int nFEval = 0;           // faces touching an own cell: the first nFEval of the GPU face order
     bool parted = false;      // built from one part of a partitioned mesh
     fg_halo_ops halo{};       // the partitioned run's transport (fg_solver_set_halo)
     void *haloSend = nullptr, *haloRecv = nullptr;
@@ -187,11 +189,11 @@ struct fg_solver {
     // primitive records before (they changed in the last update / relaxation), their gradient
     // records after (the face fluxes read both sides')
     int gradients_halo(cudaStream_t s) {
+        // one exchange per stage: the ghosts' primitive records; the gradient pass covers the own
+        // and first-layer cells, whose faces the part mesh holds
         int rc;
         if (parted && (rc = halo_exchange(FG_HALO_W, s))) return rc;
-        if ((rc = gradients(s))) return rc;
-        if (parted && (rc = halo_exchange(FG_HALO_G, s))) return rc;
-        return FG_OK;
+        return gradients(s);
     }
     // combine a per-part scalar over the parts (no-op on an unpartitioned mesh)
     int reduce(int op, double *v) {
@@ -310,6 +312,7 @@ struct SolverT : public fg_solver {
     int init(const fg::Mesh &m) override {
         n = m.nElem;
         nU = m.owned();
+        nG = m.gradient_cells();
         parted = m.nOwned >= 0;
         nSlots = m.maxFaces;
         cellCenter.assign(m.cellCenter.begin(), m.cellCenter.end());
@@ -398,7 +401,7 @@ struct SolverT : public fg_solver {
             const fg::ElemType *et = fg::elem_type_for_nodes(m.elNN[o]);
             vol[i] = m.volume[o];
             volP[i] = pow(m.volume[o], 0.3333);
-            if (i >= nU) continue;   // a ghost: records only, no faces of its own
+            if (i >= nG) continue;   // a second-layer ghost: records only, no faces of its own
             int fl = et->nFaces;
             for (int k = 0; k < et->nFaces; k++) {
                 const int f = elFc2fc[(size_t)o * 6 + k];
@@ -437,20 +440,28 @@ struct SolverT : public fg_solver {
         // then read the records of the same local face of nearby cells from nearby positions, and
         // the face kernel's lanes take nearby owners whose neighbours lie in one direction of a hex
         // brick.  A ghost owns the faces it shares with own cells where the whole mesh makes it the
-        // owner.
+        // owner.  On a part the faces touching an own cell come first (the face kernel evaluates
+        // those only); the faces among ghosts, kept for the first-layer ghosts' gradients, follow.
         std::vector<int32_t> gFace(nF, -1), slotFace(S, -1), fIdx(2 * (size_t)nF);
-        int nG = 0;
-        for (int t0 = 0; t0 < n; t0 += kFaceTile) {
-            const int t1 = std::min(n, t0 + kFaceTile);
-            for (int k = 0; k < MAXSLOT; k++)
-                for (int i = t0; i < t1; i++) {
-                    const int o = m.new2old[i];
-                    if (k >= fg::elem_type_for_nodes(m.elNN[o])->nFaces) continue;
-                    const int f = elFc2fc[(size_t)o * 6 + k];
-                    if (f >= 0 && elFcSide[(size_t)o * 6 + k] == 0) gFace[f] = nG++;
-                }
+        int nFo = 0;
+        auto touches_own = [&](int f) {
+            return m.old2new[m.fc2el[2 * f]] < nU || (m.boundCond[f] == 0 && m.old2new[m.fc2el[2 * f + 1]] < nU);
+        };
+        for (int pass = 0; pass < 2; pass++) {
+            for (int t0 = 0; t0 < n; t0 += kFaceTile) {
+                const int t1 = std::min(n, t0 + kFaceTile);
+                for (int k = 0; k < MAXSLOT; k++)
+                    for (int i = t0; i < t1; i++) {
+                        const int o = m.new2old[i];
+                        if (k >= fg::elem_type_for_nodes(m.elNN[o])->nFaces) continue;
+                        const int f = elFc2fc[(size_t)o * 6 + k];
+                        if (f >= 0 && elFcSide[(size_t)o * 6 + k] == 0 && touches_own(f) == (pass == 0))
+                            gFace[f] = nFo++;
+                    }
+            }
+            if (pass == 0) nFEval = nFo;
         }
-        if (nG != nF) return set_err(FG_ERR_MESH, "internal: face ownership does not cover every face");
+        if (nFo != nF) return set_err(FG_ERR_MESH, "internal: face ownership does not cover every face");
         // face geometry: 11 components (n[3], A, x_f - x_owner [3], x_f - x_nb [3], WALE Ls^2)
         const size_t FS = ((size_t)nF * sizeof(T) + 15) / 16 * 16 / sizeof(T);
         std::vector<T> fgeo(11 * FS, (T)0);
@@ -601,6 +612,8 @@ struct SolverT : public fg_solver {
             bytes += b->bytes;
         dm.n = n;
         dm.nU = nU;
+        dm.nG = nG;
+        dm.nFEval = nFEval;
         dm.nSlots = nSlots;
         dm.nbr = dNbr.as<int32_t>();
         dm.flags = dFlags.as<int32_t>();
@@ -757,9 +770,10 @@ struct SolverT : public fg_solver {
     int halo_exchange(int field, cudaStream_t s) override {
         if (!halo.exchange)
             return set_err(FG_ERR_ARG, "partitioned mesh: set the transport with fg_solver_set_halo first");
-        T *rec = (field == FG_HALO_W) ? dW[cur].as<T>() : dG.as<T>();
-        const int stride = (field == FG_HALO_W) ? WREC : GREC;
-        const int vpvRec = (field == FG_HALO_W) ? vpv<T>() : gvec<T>();
+        if (field != FG_HALO_W) return set_err(FG_ERR_ARG, "partitioned run: only primitive records are exchanged");
+        T *rec = dW[cur].as<T>();
+        const int stride = WREC;
+        const int vpvRec = vpv<T>();
         const int nSend = sendStart.back(), nRecv = recvStart.back();
         prof_begin(FG_K_OTHER, s);
         launch_halo_pack<T>(rec, (size_t)n, stride, vpvRec, dSendCells.as<int32_t>(), nSend, static_cast<T *>(haloSend), s);
@@ -776,7 +790,7 @@ struct SolverT : public fg_solver {
         return FG_OK;
     }
     void halo_bytes(int64_t *send, int64_t *recv) const override {
-        const int64_t rb = (int64_t)GREC * (int64_t)sizeof(T);   // the larger of the two records
+        const int64_t rb = (int64_t)WREC * (int64_t)sizeof(T);   // primitive records only
         *send = parted ? rb * sendStart.back() : 0;
         *recv = parted ? rb * recvStart.back() : 0;
     }
@@ -1163,6 +1177,7 @@ int fg_mesh_partition_info(const fg_mesh *mm, fg_partition_info *info) {
     info->nGhost = m.nElem - m.owned();
     info->nSend = m.sendStart.empty() ? 0 : m.sendStart.back();
     info->nRecv = m.recvStart.empty() ? 0 : m.recvStart.back();
+    info->nGhost1 = m.nOwned < 0 ? 0 : m.nGhost1;
     return FG_OK;
 }
 int fg_mesh_partition_maps(const fg_mesh *mm, int32_t *cellGlobal, int32_t *sendStart, int32_t *sendCells,

@@ -2,9 +2,10 @@
 
 The reference exchanges its halo faces with MPI point-to-point messages every stage
 (DP/communicate.cu) and reduces dt / the conservation sums with MPI_Allreduce.  Here each part's
-solver packs the records of its own halo cells into a device send buffer; this class moves, for
-every neighbouring part q, the slice of records that q needs and receives q's records into the
-ghost slice of the receive buffer:
+solver packs the primitive records of its own cells that other parts hold as ghosts (once per
+stage; each part computes its first-layer ghosts' gradients itself) into a device send buffer;
+this class moves, for every neighbouring part q, the slice of records that q needs and receives
+q's records into the ghost slice of the receive buffer:
 
 - an NCCL group sends the device buffers directly (peer traffic over NVLink / NVSwitch);
 - a gloo group stages them through host memory (CPU tests, or hosts without NCCL).

@@ -202,9 +202,11 @@ void fg_mesh_free(fg_mesh *m);
  * Replace the reference's METIS decomposition, local-mesh build and per-stage halo
  * communication (DP/decompose.cu:52, DP/buildLocalMesh.cu, DP/communicate.cu) for runs with one
  * GPU per part.  Part p of P owns the cells of the contiguous range [n p / P, n (p+1) / P) of the
- * mesh's device order (the Morton order of the cell centres: a compact region) and holds one
- * layer of ghost cells, its face neighbours in other parts.  The part mesh keeps every face that
- * touches an own cell with the whole mesh's orientation, geometry and boundary code.
+ * mesh's device order (the Morton order of the cell centres: a compact region) and holds two
+ * layers of ghost cells: its face neighbours in other parts, and their face neighbours outside
+ * both.  The part mesh keeps every face that touches an own or a first-layer cell with the whole
+ * mesh's orientation, geometry and boundary code, so the part computes the gradients of its
+ * first-layer ghosts itself and only primitive records cross between parts.
  *
  * fg_mesh_partition: part `part` of `nParts` of a loaded mesh, as a new mesh handle whose cells
  * are the own cells (device order) followed by the ghosts.  A solver created on it takes and
@@ -214,22 +216,25 @@ int fg_mesh_partition(const fg_mesh *m, int32_t nParts, int32_t part, fg_mesh **
 typedef struct fg_partition_info {
     int32_t nParts, part;   /* 1, 0 for a mesh that is not a part                     */
     int32_t nOwned;         /* own cells: the first nOwned cells of the part mesh      */
-    int32_t nGhost;         /* ghost cells, after the own ones                         */
+    int32_t nGhost;         /* ghost cells of both layers, after the own ones          */
     int32_t nSend, nRecv;   /* entries of the send / receive lists over all parts      */
+    int32_t nGhost1;        /* first-layer ghosts: cells [nOwned, nOwned + nGhost1)    */
 } fg_partition_info;
 int fg_mesh_partition_info(const fg_mesh *m, fg_partition_info *info);
 /* cellGlobal[nOwned + nGhost]: .neu index in the whole mesh of each cell of the part;
- * sendStart[nParts + 1], sendCells[nSend]: the own cells whose records go to part q are
- * sendCells[sendStart[q] .. sendStart[q+1]); recvStart / recvCells the same for the ghosts whose
- * records come from part q.  Both lists follow the whole mesh's device order, so the k-th record
- * part p sends to q is q's k-th ghost from p.  Any pointer may be NULL. */
+ * sendStart[nParts + 1], sendCells[nSend]: the own cells whose records go to part q (those
+ * within two face hops of q's cells) are sendCells[sendStart[q] .. sendStart[q+1]); recvStart /
+ * recvCells the same for the ghosts whose records come from part q.  Both lists follow the whole
+ * mesh's device order, so the k-th record part p sends to q is q's k-th ghost from p.  Any
+ * pointer may be NULL. */
 int fg_mesh_partition_maps(const fg_mesh *m, int32_t *cellGlobal, int32_t *sendStart, int32_t *sendCells,
                            int32_t *recvStart, int32_t *recvCells);
 
 /* Transport of a partitioned run (the caller's NCCL / MPI / shared memory).  Per RK stage the
- * solver exchanges the primitive records (FG_HALO_W) of the halo cells before the gradient pass
- * and their gradient records (FG_HALO_G) after it; the dt (every adaptDtItr steps) and the
- * conservation integral are combined with allreduce.
+ * solver exchanges the primitive records (FG_HALO_W) of the ghost cells once, before the gradient
+ * pass (FG_HALO_G, the gradient records, is not exchanged: each part computes its first-layer
+ * ghosts' gradients); the dt (every adaptDtItr steps) and the conservation integral are combined
+ * with allreduce.
  *   exchange(ctx, field, recordBytes, stream): when called, sendBuf holds the nSend records of
  *     `field` (recordBytes each, in send-list order) and every earlier kernel on `stream` has
  *     finished.  The callee sends records [sendStart[q], sendStart[q+1]) to part q, receives part

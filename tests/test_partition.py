@@ -1,7 +1,9 @@
 """Space-filling-curve partition of a mesh (host C++ through the C ABI; no GPU needed): the parts'
-own cells cover the mesh once, each part keeps every face of its own cells with the whole mesh's
-orientation and geometry, its ghosts are exactly the other parts' face neighbours, and the send
-list of part p to q matches the receive list of q from p record for record."""
+own cells cover the mesh once; each part's first ghost layer is exactly the other parts' face
+neighbours of its own cells and its second layer their further neighbours; the part keeps every
+face of its own and first-layer cells with the whole mesh's orientation and geometry; and the
+send list of part p to q (p's cells within two face hops of q's) matches the receive list of q
+from p record for record."""
 import math
 
 import numpy as np
@@ -62,25 +64,39 @@ def test_partition_maps(kind, P, tmp_path):
         # per-cell data is the whole mesh's
         assert np.array_equal(a["volume"], ga["volume"][cg])
         assert np.array_equal(a["cellCenter"], ga["cellCenter"][cg])
-        # faces: exactly those touching an own cell, in whole-mesh order, same orientation / geometry
-        mine = owner_part[gown] == p
-        mine |= inner & (owner_part[np.where(inner, gnb, 0)] == p)
+        n1 = info["nGhost1"]
+        # ghost layers: the other parts' face neighbours of own cells, then their neighbours outside
+        # both, each sorted by device order
+        nbr = [set() for _ in range(n)]
+        for f in np.flatnonzero(inner):
+            nbr[gown[f]].add(int(gnb[f]))
+            nbr[gnb[f]].add(int(gown[f]))
+        own_set = set(cg[:m.n_owned].tolist())
+        layer1 = set()
+        for x in own_set:
+            layer1 |= {y for y in nbr[x] if owner_part[y] != p}
+        layer2 = set()
+        for x in layer1:
+            layer2 |= {y for y in nbr[x] if y not in own_set and y not in layer1}
+        g1, g2 = cg[m.n_owned:m.n_owned + n1], cg[m.n_owned + n1:]
+        assert set(g1.tolist()) == layer1 and len(g1) == len(layer1)
+        assert set(g2.tolist()) == layer2 and len(g2) == len(layer2)
+        old2new = np.argsort(new2old)
+        assert np.all(np.diff(old2new[g1]) > 0) and np.all(np.diff(old2new[g2]) > 0)
+        # faces: exactly those touching an own or first-layer cell, in whole-mesh order, same
+        # orientation / geometry
+        inner_cells = own_set | layer1
+        mine = np.array([int(gown[f]) in inner_cells or (bool(inner[f]) and int(gnb[f]) in inner_cells)
+                         for f in range(len(gown))])
         sel = np.flatnonzero(mine)
         own, nb = _faces_key(a, cg)
         assert np.array_equal(own, gown[sel]) and np.array_equal(nb, gnb[sel])
         for k in ("n", "area", "fcCenter", "nbShift", "boundCond"):
             assert np.array_equal(a[k], ga[k][sel]), k
-        # ghosts: the other parts' neighbours of own cells, sorted by device order
-        ghosts = cg[m.n_owned:]
-        nbrs = set()
-        for f in sel[inner[sel]]:
-            for x, y in ((gown[f], gnb[f]), (gnb[f], gown[f])):
-                if owner_part[x] == p and owner_part[y] != p:
-                    nbrs.add(int(y))
-        assert set(ghosts.tolist()) == nbrs and len(ghosts) == len(nbrs)
-        old2new = np.argsort(new2old)
-        assert np.all(np.diff(old2new[ghosts]) > 0)
-        assert np.array_equal(mp["recv_cells"], np.arange(m.n_owned, m.n_elem))
+        # received: every ghost once, grouped by owning part, in device order
+        rc = mp["recv_cells"]
+        assert np.array_equal(np.sort(rc), np.arange(m.n_owned, m.n_elem))
+        assert np.all(np.diff(old2new[cg[rc]]) > 0)
         assert mp["recv_start"][p] == mp["recv_start"][p + 1] and mp["send_start"][p] == mp["send_start"][p + 1]
     # what p sends to q is what q receives from p, in the same order
     for p in range(P):
@@ -101,7 +117,8 @@ def test_single_part_is_the_mesh(tmp_path):
 
 def test_whole_mesh_reports_one_part(tmp_path):
     g = _mesh("tets", tmp_path)
-    assert g.part_info == {"nParts": 1, "part": 0, "nOwned": g.n_elem, "nGhost": 0, "nSend": 0, "nRecv": 0}
+    assert g.part_info == {"nParts": 1, "part": 0, "nOwned": g.n_elem, "nGhost": 0, "nSend": 0, "nRecv": 0,
+                           "nGhost1": 0}
     mp = g.partition_maps()
     assert np.array_equal(mp["cell_global"], np.arange(g.n_elem))
 
