@@ -783,7 +783,7 @@ def run_partitioned(args, rank, world, local_rank, dist):
         dtype="fp32 face math + fp64 state/RK (mixed)", data="synthetic",
         config={"workload": f"tgv_les_wale_{NCELL_SIDE}^3_hex_periodic", "cells": nE, "rk_stages": case.rkSteps,
                 "parallelism": f"partitioned mesh, {world} parts (space-filling-curve ranges), NCCL halo per stage",
-                "ghost_cells_total": int(halo_cells.item()), "halo_exchanges_per_step": 2 * case.rkSteps},
+                "ghost_cells_total": int(halo_cells.item()), "halo_exchanges_per_step": case.rkSteps},
         e2e={"value": nE * case.rkSteps * e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
              "h2d_bytes_per_step": nE * 80, "d2h_bytes_per_step": nE * 80, "steps": e2e_steps},
         gpu_launches=launches, clocks=cl)
