@@ -119,7 +119,8 @@ class Mesh:
 
     def partition(self, n_parts: int, part: int) -> "Mesh":
         """Part `part` of `n_parts` (contiguous ranges of the Morton device order): own cells first,
-        then one layer of ghost cells; the returned mesh is independent of this one."""
+        then two layers of ghost cells (the other parts' face neighbours, then theirs); the returned
+        mesh is independent of this one."""
         h = C.c_void_p()
         check(lib().fg_mesh_partition(self._h, int(n_parts), int(part), C.byref(h)))
         return Mesh(h)
