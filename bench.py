@@ -300,6 +300,7 @@ def run_ours(args, rank, world, local_rank, dist):
     flux_ms = (fl["ms"] + ga["ms"]) / fl["launches"]
     achieved = bf * nE / (flux_ms / 1e3) / 1e9
     traffic = None
+    dram = None
     tr_path = ROOT / "profiles" / "flux_traffic.json"
     if tr_path.exists():
         try:
@@ -307,8 +308,18 @@ def run_ours(args, rank, world, local_rank, dist):
             traffic = t.get("mixed_bytes_per_cell", None)
             if traffic is not None:
                 traffic = traffic * nE
+            # the DRAM bytes each kernel moves (committed ncu capture, per cell) over its CUDA-event
+            # time here: the measured-traffic reading of the flux / gather bar
+            dram = {}
+            for key, kind in (("k_face<float>", "face"), ("k_gather<float>", "gather"), ("k_grad<float>", "grad")):
+                bpc = t.get(f"{kind}_bytes_per_cell")
+                src = prof["flux" if kind == "face" else kind]
+                if bpc is None or not src["launches"]:
+                    continue
+                gbs = bpc * nE / (src["ms"] / src["launches"] / 1e3) / 1e9
+                dram[key] = {"bytes_per_cell": bpc, "gbs": gbs, "frac": gbs / peak}
         except Exception:
-            traffic = None
+            traffic, dram = None, None
     # whole path: per-GPU cell-stages/s x algorithmic bytes per cell-stage (both passes)
     whole_frac = (value / world) * (bg + bf) / 1e9 / peak
     out = dict(
@@ -330,7 +341,9 @@ def run_ours(args, rank, world, local_rank, dist):
                   "traffic": traffic, "kernel": "k_face<float> + k_gather<float> (face flux, owner-side gather + RK)",
                   "algorithmic_bytes_per_launch": bf * nE, "avg_launch_ms": flux_ms,
                   "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                  "whole_path_frac": whole_frac},
+                  "whole_path_frac": whole_frac,
+                  "traffic_frac": (traffic / (flux_ms / 1e3) / 1e9 / peak) if traffic else None,
+                  "dram_measured": dram},
         kernels={k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]} for k, v in prof.items()},
         kernels_fp64={k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]} for k, v in prof64.items()},
         clocks=cl,
