@@ -464,14 +464,20 @@ struct InRelax {
 #ifndef FG_THERM_MINBLOCKS
 #define FG_THERM_MINBLOCKS 6
 #endif
-// the same for the chemical-first instantiations (kOrd true: Gibbs and thermal Newton): 4 blocks
-// (128 registers, a few spilled, against 156-196 uncapped) measured 2.81 -> 1.99 ms (FP64 Newton)
-// and 0.81 -> 0.66 ms (surrogate + polish) per relaxation on the 96^3 two-phase workload
+// the same for the chemical-first instantiations (kOrd true: Gibbs and thermal Newton).  Without
+// the surrogate 6 blocks (85 registers) measured 0.770 -> 0.730 ms per relaxation on a 64^3
+// two-phase box (39 % chemical cells) and 1.321 -> 1.157 ms on the 4 M-tet bubble (almost all
+// thermal) against 4 blocks (5 and 7 were slower on the box); uncapped (156-196 registers) was
+// 2.81 ms against 1.99 at 4 blocks on the 96^3 box.  With the surrogate's polish path 4 blocks
+// (128 registers) measured 0.81 -> 0.66 ms against uncapped on that box.
 #ifndef FG_CHEM_MINBLOCKS
-#define FG_CHEM_MINBLOCKS 4
+#define FG_CHEM_MINBLOCKS 6
+#endif
+#ifndef FG_CHEM_SG_MINBLOCKS
+#define FG_CHEM_SG_MINBLOCKS 4
 #endif
 template <typename T, bool kSG, bool kLog, bool kOrd>
-__global__ void __launch_bounds__(128, kOrd ? FG_CHEM_MINBLOCKS : FG_THERM_MINBLOCKS) k_relax(int n, double *U, T *W, size_t wStride, const PhysD D, const RelaxParams R,
+__global__ void __launch_bounds__(128, kOrd ? (kSG ? FG_CHEM_SG_MINBLOCKS : FG_CHEM_MINBLOCKS) : FG_THERM_MINBLOCKS) k_relax(int n, double *U, T *W, size_t wStride, const PhysD D, const RelaxParams R,
                                                int32_t *counters, const SurrogateDev S, const RelaxLog Lg,
                                                const int32_t *order, const int32_t *nChem, const float4 *pred,
                                                const int32_t *hullOk) {
