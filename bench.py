@@ -782,7 +782,8 @@ def run_partitioned(args, rank, world, local_rank, dist):
     for _ in range(e2e_steps):
         s.set_state_async(Uin.numpy(), stream=stream.cuda_stream)
         s.step(stream=stream.cuda_stream)
-        s.get_state(Uout.numpy(), stream=stream.cuda_stream)
+        s.get_state_async(Uout.numpy(), stream=stream.cuda_stream)
+    s.state_join(stream=stream.cuda_stream)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = rank_max(e0.elapsed_time(e1), dist, f"cuda:{dev}")
@@ -859,7 +860,8 @@ def main():
     ap.add_argument("--no-mesh-timing", action="store_true", help="skip timing the host vs GPU mesh pre-processor")
     ap.add_argument("--no-jet", action="store_true", help="skip the 40 M-cell liquid jet")
     ap.add_argument("--partition", action="store_true",
-                    help="N > 1: one partitioned mesh over the N GPUs (NCCL halo) instead of N replicas")
+                    help="one partitioned mesh over the N GPUs (NCCL halo) instead of N replicas (launched "
+                         "through torch.distributed.run, N = 1 included)")
     ap.add_argument("--jet-steps", type=int, default=20, help="timed steps per path of the jet (the configuration: 200)")
     ap.add_argument("--jet-host-mesh", action="store_true", help="also time the host pre-processor on the jet mesh")
     ap.add_argument("--n", type=int, default=None, help="cells per side of the TGV cube (default 128)")
@@ -877,7 +879,9 @@ def main():
             print(json.dumps(run_reference(args)), flush=True)
         return
     dist = None
-    if world > 1:
+    # --partition needs the process group even on one GPU (one part, no neighbours: the partitioned
+    # code path with nothing to exchange)
+    if world > 1 or args.partition:
         import datetime
         import torch
         import torch.distributed as D
