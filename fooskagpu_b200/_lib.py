@@ -137,6 +137,7 @@ SIGNATURES = {
     "fg_surrogate_set_norm": (C.c_int, [VP, PF]),
     "fg_surrogate_predict": (C.c_int, [VP, PF, i32, PF, PI]),
     "fg_solver_set_surrogate": (C.c_int, [VP, VP, f64, i32]),
+    "fg_solver_set_surrogate_pass": (C.c_int, [VP, i32]),
     "fg_relax_log": (C.c_int, [VP, i64]),
     "fg_check_state": (C.c_int, [VP, PI]),
     "fg_checkpoint_write": (C.c_int, [VP, C.c_char_p]),

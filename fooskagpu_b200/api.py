@@ -284,6 +284,15 @@ class Solver:
         self._sg = sg
         check(lib().fg_solver_set_surrogate(self._h, sg._h if sg is not None else None, rel_tol, polish_iters))
 
+    def set_surrogate_pass(self, mode: str = "auto") -> None:
+        """Where the surrogate's polish runs: "fused" (inside the relaxation kernel), "separate" (a
+        pass of its own before it) or "auto" (chosen per relaxation from the chemical cells of an
+        earlier one).  The relaxed states are bitwise the same for all three."""
+        modes = {"auto": 0, "fused": 1, "separate": 2}
+        if mode not in modes:
+            raise ValueError(f"surrogate pass mode {mode!r}: one of {sorted(modes)}")
+        check(lib().fg_solver_set_surrogate_pass(self._h, modes[mode]))
+
     def relax_log(self, capacity: int) -> None:
         """Log chemical Newton solves as surrogate training samples (0 turns the log off)."""
         check(lib().fg_relax_log(self._h, int(capacity)))

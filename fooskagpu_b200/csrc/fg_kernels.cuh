@@ -203,6 +203,7 @@ struct RelaxOrder {
     float4 *pred;        // [n] surrogate prediction of the chemical cell order[i]
     int32_t *hullOk;     // [n] its input is inside the training hull
     int32_t *tcErr;      // [1] a tensor-core completion wait timed out
+    int polishPass;      // with the surrogate: polish in k_relax_polish before the relaxation kernel
 };
 int relax_order_blocks(int n);
 // returns the number of kernels launched

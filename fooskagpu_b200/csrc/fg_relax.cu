@@ -434,9 +434,10 @@ __global__ void k_relax_order(int n, const uint8_t *isChem, const int32_t *block
 
 
 // kSG / kLog: instantiated with the surrogate path / the solve log; the plain instantiation
-// carries none of their code (and none of their registers).  kOrd: thread i relaxes cell
-// order[i], chemical when i < *nChem (k_relax_order); otherwise thread i relaxes cell i and
-// decides the branch itself.
+// carries none of their code (and none of their registers).  kPass (with kSG): the surrogate's
+// polish ran before, in k_relax_polish, and the cells it accepted are skipped; otherwise the
+// polish runs here.  kOrd: thread i relaxes cell order[i], chemical when i < *nChem
+// (k_relax_order); otherwise thread i relaxes cell i and decides the branch itself.
 // surrogate input of the relaxation: chemical cell order[i], i < *nChem
 struct InRelax {
     const double *U;
@@ -469,18 +470,77 @@ struct InRelax {
 // two-phase box (39 % chemical cells) and 1.321 -> 1.157 ms on the 4 M-tet bubble (almost all
 // thermal) against 4 blocks (5 and 7 were slower on the box); uncapped (156-196 registers) was
 // 2.81 ms against 1.99 at 4 blocks on the 96^3 box.  With the surrogate's polish path 4 blocks
-// (128 registers) measured 0.81 -> 0.66 ms against uncapped on that box.
+// (128 registers) measured 0.81 -> 0.66 ms against uncapped on that box.  The same budget serves
+// k_relax_polish, the surrogate's polish as a pass of its own.
 #ifndef FG_CHEM_MINBLOCKS
 #define FG_CHEM_MINBLOCKS 6
 #endif
 #ifndef FG_CHEM_SG_MINBLOCKS
 #define FG_CHEM_SG_MINBLOCKS 4
 #endif
-template <typename T, bool kSG, bool kLog, bool kOrd>
-__global__ void __launch_bounds__(128, kOrd ? (kSG ? FG_CHEM_SG_MINBLOCKS : FG_CHEM_MINBLOCKS) : FG_THERM_MINBLOCKS) k_relax(int n, double *U, T *W, size_t wStride, const PhysD D, const RelaxParams R,
+
+// hullOk[i] of a chemical cell whose polished surrogate solution k_relax_polish accepted
+constexpr int32_t kPolished = 2;
+
+// Surrogate pass over the chemical cells (order[0 .. *nChem)), before k_relax: each cell whose
+// network input lies inside the training hull (hullOk[i] = 1, k_sg_tc) is polished from the
+// network's prediction pred[i]; an accepted cell gets its relaxed state (U and its W record) and
+// hullOk[i] = kPolished, and k_relax leaves it alone.  Running the polish in its own kernel keeps
+// its register budget off the thermal Newton's.  Grid-stride over the resident blocks.  Counts
+// the polish steps (accepted or not) as Newton iterations, the accepted cells and their polish
+// steps.  Its results are bitwise those of the polish inside k_relax (same arithmetic per cell).
+template <typename T>
+__global__ void __launch_bounds__(128, FG_CHEM_SG_MINBLOCKS) k_relax_polish(int n, double *U, T *W, size_t wStride,
+                                               const PhysD D, const RelaxParams R, int32_t *counters,
+                                               const SurrogateDev S, const int32_t *order, const int32_t *nChem,
+                                               const float4 *pred, int32_t *hullOk) {
+    const int m = *nChem;
+    const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
+    // base is the same for every thread of the block: the warp collectives below see full warps
+    for (int base = blockIdx.x * blockDim.x; base < m; base += gridDim.x * blockDim.x) {
+        const int i = base + threadIdx.x;
+        int used = 0, pits = 0;
+        if (i < m && hullOk[i]) {
+            const int c = order[i];
+            double u[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
+            double rm, re, ag;
+            chem_mixture(R, u, &rm, &re, &ag);
+            const float4 p4 = pred[i];
+            const float pr[4] = {p4.x, p4.y, p4.z, p4.w};
+            used = chem_polish(R, h, u, pr, rm, re, S.relTol, S.polishIters, &pits);
+            if (used) {
+                U[(size_t)0 * n + c] = u[0];
+                U[(size_t)1 * n + c] = u[1];
+                U[(size_t)2 * n + c] = u[2];
+                U[(size_t)6 * n + c] = u[6];
+                U[(size_t)7 * n + c] = u[7];
+                U[(size_t)9 * n + c] = u[9];
+                T w[NP];
+                cons2prim_d(D, u, w);
+                rec_store<T, NP>(W, wStride, c, w);
+                hullOk[i] = kPolished;
+            }
+        }
+        const unsigned maskS = __ballot_sync(0xffffffffu, used);
+        const int itsW = __reduce_add_sync(0xffffffffu, pits);
+        const int polW = __reduce_add_sync(0xffffffffu, used ? pits : 0);
+        if ((threadIdx.x & 31) == 0) {
+            if (itsW) atomicAdd(&counters[3], itsW);
+            if (maskS) atomicAdd(&counters[4], __popc(maskS));
+            if (polW) atomicAdd(&counters[6], polW);
+        }
+    }
+}
+
+template <typename T, bool kSG, bool kLog, bool kOrd, bool kPass = false>
+__global__ void __launch_bounds__(128, kOrd ? ((kSG && !kPass) ? FG_CHEM_SG_MINBLOCKS : FG_CHEM_MINBLOCKS)
+                                            : FG_THERM_MINBLOCKS) k_relax(int n, double *U, T *W, size_t wStride, const PhysD D, const RelaxParams R,
                                                int32_t *counters, const SurrogateDev S, const RelaxLog Lg,
                                                const int32_t *order, const int32_t *nChem, const float4 *pred,
                                                const int32_t *hullOk) {
+    constexpr bool kPolish = kSG && !kPass;   // the polish runs in this kernel
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool act = i < n;
     const int c = (kOrd && act) ? order[i] : i;
@@ -488,43 +548,41 @@ __global__ void __launch_bounds__(128, kOrd ? (kSG ? FG_CHEM_SG_MINBLOCKS : FG_C
     const Ph h[2] = {{R.gam[0], R.pinf[0], R.cp[0], R.eta[0]}, {R.gam[1], R.pinf[1], R.cp[1], R.eta[1]}};
     double u[NV];
     double rm = 0, re = 0, ag = 0;
-    bool want = false;
     if (act) {
-#pragma unroll
-        for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
         // kOrd: cells ordered chemical-first (chemFlag == 1); otherwise every cell is thermal
         // (chemFlag != 1), and the chemical solver is compiled out of this instantiation
         if (kOrd) chem = i < *nChem;
-        if (chem && (kSG || kLog)) {
-            chem_mixture(R, u, &rm, &re, &ag);
-            // the network's prediction for this cell (k_sg_tc over the chemical cells) if its
-            // input is inside the training hull
-            if (kSG) want = hullOk[i] != 0;
-        }
+        // relaxed already by the surrogate pass
+        if (kSG && kPass && chem) used = hullOk[i] == kPolished;
     }
-    if (act) {
-        if (kSG && want) {
+    if (act && !used) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) u[v] = U[(size_t)v * n + c];
+        if (chem && (kPolish || kLog)) chem_mixture(R, u, &rm, &re, &ag);
+        // the network's prediction for this cell (k_sg_tc over the chemical cells) if its input
+        // is inside the training hull
+        if (kPolish && chem && hullOk[i] != 0) {
             const float4 p4 = pred[i];
             const float pr[4] = {p4.x, p4.y, p4.z, p4.w};
             used = chem_polish(R, h, u, pr, rm, re, S.relTol, S.polishIters, &pits);
         }
         if (!used) {
             ab = (kOrd && chem) ? chem_cell(R, h, u, &its) : therm_cell(R, h, u, &its);
-            if (kLog && chem && !ab) {
-                // training sample: (rho, e, Y) before the solve -> (p, T, alpha, Y_eq) after it
-                const unsigned long long k = atomicAdd(Lg.count, 1ULL);
-                if (k < (unsigned long long)Lg.cap) {
-                    const double a0 = fmin(fmax(R.avfMin / 100, u[0]), 1 - R.avfMin / 100);
-                    const double rL = u[1] / a0, eL = u[6] / u[1];
-                    float *x = Lg.X + k * 3, *y = Lg.Y + k * 4;
-                    x[0] = (float)rm;
-                    x[1] = (float)(re / rm);
-                    x[2] = (float)(ag / rm);
-                    y[0] = (float)p_of(h[0], rL, eL);
-                    y[1] = (float)t_of(h[0], rL, eL);
-                    y[2] = (float)a0;
-                    y[3] = (float)(u[9] / rm);
-                }
+        }
+        if (kLog && chem && !used && !ab) {
+            // training sample: (rho, e, Y) before the solve -> (p, T, alpha, Y_eq) after it
+            const unsigned long long k = atomicAdd(Lg.count, 1ULL);
+            if (k < (unsigned long long)Lg.cap) {
+                const double a0 = fmin(fmax(R.avfMin / 100, u[0]), 1 - R.avfMin / 100);
+                const double rL = u[1] / a0, eL = u[6] / u[1];
+                float *x = Lg.X + k * 3, *y = Lg.Y + k * 4;
+                x[0] = (float)rm;
+                x[1] = (float)(re / rm);
+                x[2] = (float)(ag / rm);
+                y[0] = (float)p_of(h[0], rL, eL);
+                y[1] = (float)t_of(h[0], rL, eL);
+                y[2] = (float)a0;
+                y[3] = (float)(u[9] / rm);
             }
         }
         its += pits;   // polish steps count as Newton iterations (accepted or not)
@@ -542,10 +600,11 @@ __global__ void __launch_bounds__(128, kOrd ? (kSG ? FG_CHEM_SG_MINBLOCKS : FG_C
     const unsigned mask = __ballot_sync(0xffffffffu, act && chem);
     const unsigned maskT = __ballot_sync(0xffffffffu, act && !chem);
     const unsigned maskA = __ballot_sync(0xffffffffu, act && ab);
-    const unsigned maskS = __ballot_sync(0xffffffffu, act && used);
+    // accepted cells and their polish steps: counted here when the polish ran here
+    const unsigned maskS = kPolish ? __ballot_sync(0xffffffffu, act && used) : 0u;
     const unsigned maskF = __ballot_sync(0xffffffffu, act && chem && kSG && !used);
     const int itsW = __reduce_add_sync(0xffffffffu, its);
-    const int polW = kSG ? __reduce_add_sync(0xffffffffu, used ? pits : 0) : 0;   // polish steps of accepted cells
+    const int polW = kPolish ? __reduce_add_sync(0xffffffffu, used ? pits : 0) : 0;
     if ((threadIdx.x & 31) == 0) {
         if (maskT) atomicAdd(&counters[0], __popc(maskT));
         if (mask) atomicAdd(&counters[1], __popc(mask));
@@ -567,11 +626,20 @@ static void launch_relax_k(int n, double *U, T *W, size_t wStride, const PhysD &
     const int32_t *order = O ? O->order : nullptr, *nChem = O ? O->total : nullptr;
     const float4 *pred = O ? O->pred : nullptr;
     const int32_t *hull = O ? O->hullOk : nullptr;
-    if (kOrd && S.enabled && lg)
-        k_relax<T, true, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
-    else if (kOrd && S.enabled)
-        k_relax<T, true, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
-    else if (lg)
+    if constexpr (kOrd) {
+        // the surrogate runs only with the chemical-first order; the logged instantiation keeps
+        // the polish inside (launch_relax runs no separate pass with the log on)
+        if (S.enabled) {
+            if (lg)
+                k_relax<T, true, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
+            else if (O->polishPass)
+                k_relax<T, true, false, kOrd, true><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
+            else
+                k_relax<T, true, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
+            return;
+        }
+    }
+    if (lg)
         k_relax<T, false, true, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
     else
         k_relax<T, false, false, kOrd><<<nb, 128, 0, s>>>(n, U, W, wStride, D, R, counters, S, L, order, nChem, pred, hull);
@@ -596,6 +664,11 @@ int launch_relax(int n, double *U, T *W, size_t wStride, const PhysD &D, const R
         k_sg_tc<InRelax><<<std::min(tiles, 148 * 4), 128, TC_SMEM, s>>>(S, S.pack, InRelax{U, n, O.order, O.total, R},
                                                                         O.pred, O.hullOk, O.tcErr);
         k++;
+        if (O.polishPass && L.count == nullptr) {
+            k_relax_polish<T><<<std::min((n + 127) / 128, 148 * FG_CHEM_SG_MINBLOCKS), 128, 0, s>>>(
+                n, U, W, wStride, D, R, counters, S, O.order, O.total, O.pred, O.hullOk);
+            k++;
+        }
     }
     launch_relax_k<T, true>(n, U, W, wStride, D, R, counters, S, L, &O, s);
     return k;

@@ -78,7 +78,16 @@ struct fg_solver {
             if (e) cudaEventDestroy(e);
         if (evGathered) cudaEventDestroy(evGathered);
         if (downStream) cudaStreamDestroy(downStream);
+        if (hCntPrev) cudaFreeHost(hCntPrev);
+        if (evCnt) cudaEventDestroy(evCnt);
     }
+    // where the surrogate's polish runs (FG_SG_PASS_*).  Automatic: the relaxation counters of
+    // the last surrogate relaxation, copied to pinned host memory behind it (created on the first
+    // one), choose the next one's form once they have arrived
+    int sgPass = FG_SG_PASS_AUTO;
+    int32_t *hCntPrev = nullptr;
+    cudaEvent_t evCnt = nullptr;
+    bool cntValid = false;
     // asynchronous uploads copy on their own stream into their own staging buffer, so the copy of
     // the next state overlaps the work queued before it (created on the first asynchronous upload)
     cudaStream_t copyStream = nullptr;
@@ -271,6 +280,10 @@ __global__ void k_field_vars(int n, const double *__restrict__ U, const T *__res
     o[11] = u[9];
     o[12] = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
 }
+
+// automatic surrogate polish pass: a separate pass when fewer than one cell in kSparseChemInv of
+// the previous surrogate relaxation was chemical
+constexpr int kSparseChemInv = 10;
 
 template <typename T>
 struct SolverT : public fg_solver {
@@ -876,13 +889,39 @@ struct SolverT : public fg_solver {
             S.polishIters = sgIters;
         }
         RelaxLog L{logX.as<float>(), logY.as<float>(), logCap > 0 ? logCnt.as<unsigned long long>() : nullptr, logCap};
+        // with the surrogate, where its polish runs: inside the relaxation kernel, which then
+        // needs the polish's register budget (4 resident blocks), or as a pass of its own before
+        // it, which costs a launch and a second read of the chemical cells' states but leaves the
+        // relaxation kernel the thermal Newton's budget (6 blocks).  Measured: the separate pass
+        // is faster when few cells are chemical (4 M-tet bubble, about 1,000 chemical cells: 2.51e9
+        // -> 2.60e9 cell-updates/s), the polish inside when many are (96^3 box, 39 % chemical:
+        // 0.61 against 0.75 ms per relaxation).  The results are bitwise the same either way, so
+        // the automatic choice may use whatever counters have reached the host.
+        int pass = sgPass == FG_SG_PASS_SEPARATE;
+        if (sg && sgPass == FG_SG_PASS_AUTO) {
+            if (!hCntPrev) {
+                FG_CUDA_TRY(cudaHostAlloc((void **)&hCntPrev, 8 * sizeof(int32_t), cudaHostAllocDefault));
+                FG_CUDA_TRY(cudaEventCreateWithFlags(&evCnt, cudaEventDisableTiming));
+            } else if (cntValid) {
+                const cudaError_t q = cudaEventQuery(evCnt);
+                if (q == cudaSuccess) pass = (int64_t)hCntPrev[1] * kSparseChemInv < (int64_t)nU;
+                else if (q == cudaErrorNotReady) (void)cudaGetLastError();   // not an error: clear it
+                else return set_err(FG_ERR_CUDA, std::string("relaxation counters: ") + cudaGetErrorString(q));
+            }
+        }
         const RelaxOrder O{dOrdFlag.as<uint8_t>(), dOrdCnt.as<int32_t>(), dOrdOff.as<int32_t>(), dOrder.as<int32_t>(),
-                           dOrdTotal.as<int32_t>(), dPred.as<float4>(), dHullOk.as<int32_t>(), dTcErr.as<int32_t>()};
+                           dOrdTotal.as<int32_t>(), dPred.as<float4>(), dHullOk.as<int32_t>(), dTcErr.as<int32_t>(),
+                           pass};
         prof_begin(FG_K_RELAX, s);
         const int k = launch_relax<T>(nU, dU.as<double>(), dW[cur].as<T>(), (size_t)n, D, R, dCnt.as<int32_t>(), S, L, O, s);
         prof_end(s);
         launches += k - 1;
         FG_LAUNCH_CHECK("relaxation");
+        if (sg && sgPass == FG_SG_PASS_AUTO) {
+            FG_CUDA_TRY(cudaMemcpyAsync(hCntPrev, dCnt.p, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            FG_CUDA_TRY(cudaEventRecord(evCnt, s));
+            cntValid = true;
+        }
         if (st) {
             FG_CUDA_TRY(cudaStreamSynchronize(s));
             return relax_counts(st);
@@ -1324,6 +1363,14 @@ int fg_solver_set_surrogate(fg_solver *s, const fg_surrogate *g, double relTol, 
     s->sg = g;
     s->sgTol = relTol;
     s->sgIters = polishIters;
+    return FG_OK;
+}
+int fg_solver_set_surrogate_pass(fg_solver *s, int32_t mode) {
+    FG_ENTER(s);
+    if (mode != FG_SG_PASS_AUTO && mode != FG_SG_PASS_FUSED && mode != FG_SG_PASS_SEPARATE)
+        return set_err(FG_ERR_ARG, "fg_solver_set_surrogate_pass: mode is FG_SG_PASS_AUTO, _FUSED or _SEPARATE");
+    s->sgPass = mode;
+    s->cntValid = false;
     return FG_OK;
 }
 int fg_relax_stats_read(fg_solver *s, fg_relax_stats *stats) {

@@ -364,6 +364,15 @@ int fg_surrogate_predict(fg_surrogate *g, const float *X, int32_t n, float *Y, i
 /* attach (g != NULL) or detach the surrogate used by fg_relaxation / fg_step; g must outlive the
  * attachment and live on the solver's device */
 int fg_solver_set_surrogate(fg_solver *s, const fg_surrogate *g, double relTol, int32_t polishIters);
+/* where the attached surrogate's polish runs (no counterpart in the reference; a tuning knob):
+ * FG_SG_PASS_FUSED inside the relaxation kernel (faster when many cells are chemical),
+ * FG_SG_PASS_SEPARATE as a pass of its own before it (faster when few are), FG_SG_PASS_AUTO
+ * (default) chooses per relaxation from the chemical cells of an earlier one (separate below
+ * 10 %).  The relaxed states and counters are bitwise the same for all three. */
+#define FG_SG_PASS_AUTO 0
+#define FG_SG_PASS_FUSED 1
+#define FG_SG_PASS_SEPARATE 2
+int fg_solver_set_surrogate_pass(fg_solver *s, int32_t mode);
 /* log of chemical Newton solves as surrogate training samples: capacity 0 turns it off;
  * fg_relax_log_read copies min(logged, cap) samples (X [][3], Y [][4], order not defined) */
 int fg_relax_log(fg_solver *s, int64_t capacity);

@@ -232,3 +232,35 @@ def test_save_and_load(box, trained, data, tmp_path):
         s.close()
     assert np.array_equal(out[0], out[1])
     h.close()
+
+
+def test_polish_pass_forms_agree_bitwise(box, trained):
+    """The surrogate's polish inside the relaxation kernel, as a pass of its own before it, and the
+    automatic choice between the two give bitwise the same states and relaxation counters, in FP64
+    and mixed precision, for one relaxation and over steps."""
+    from fooskagpu_b200._lib import lib
+    m, c, cc = box
+    g = trained[0]
+    U = cases.perturbed_two_phase_ic(c, cc, seed=14, vel=25.0)
+    for prec in ("fp64", "mixed"):
+        out = {}
+        for mode in ("fused", "separate", "auto"):
+            s = Solver(m, c, precision=prec)
+            s.set_state(U)
+            s.set_surrogate(g, REL_TOL, POLISH)
+            s.set_surrogate_pass(mode)
+            st = [s.relaxation()]
+            for _ in range(4):
+                s.step()
+                st.append(s.relax_stats())
+            out[mode] = (s.get_state(), st)
+            if mode == "auto":
+                with pytest.raises(ValueError):
+                    s.set_surrogate_pass("inline")
+                assert lib().fg_solver_set_surrogate_pass(s._h, 3) != 0
+            s.close()
+        U0, st0 = out["fused"]
+        assert st0[0]["nSurrogate"] > 0.9 * st0[0]["nChem"] > 0, st0[0]
+        for mode in ("separate", "auto"):
+            assert out[mode][1] == st0, (prec, mode)
+            assert np.array_equal(out[mode][0], U0), (prec, mode)
