@@ -902,11 +902,16 @@ struct SolverT : public fg_solver {
             if (!hCntPrev) {
                 FG_CUDA_TRY(cudaHostAlloc((void **)&hCntPrev, 8 * sizeof(int32_t), cudaHostAllocDefault));
                 FG_CUDA_TRY(cudaEventCreateWithFlags(&evCnt, cudaEventDisableTiming));
-            } else if (cntValid) {
+            } else if (cntValid && cudaPeekAtLastError() == cudaSuccess) {
                 const cudaError_t q = cudaEventQuery(evCnt);
-                if (q == cudaSuccess) pass = (int64_t)hCntPrev[1] * kSparseChemInv < (int64_t)nU;
-                else if (q == cudaErrorNotReady) (void)cudaGetLastError();   // not an error: clear it
-                else return set_err(FG_ERR_CUDA, std::string("relaxation counters: ") + cudaGetErrorString(q));
+                if (q == cudaSuccess) {
+                    pass = (int64_t)hCntPrev[1] * kSparseChemInv < (int64_t)nU;
+                } else if (q == cudaErrorNotReady) {
+                    // not an error: clear it where the query itself left it as the last error
+                    if (cudaPeekAtLastError() == cudaErrorNotReady) (void)cudaGetLastError();
+                } else {
+                    return set_err(FG_ERR_CUDA, std::string("relaxation counters: ") + cudaGetErrorString(q));
+                }
             }
         }
         const RelaxOrder O{dOrdFlag.as<uint8_t>(), dOrdCnt.as<int32_t>(), dOrdOff.as<int32_t>(), dOrder.as<int32_t>(),
