@@ -368,7 +368,9 @@ int fg_solver_set_surrogate(fg_solver *s, const fg_surrogate *g, double relTol, 
  * FG_SG_PASS_FUSED inside the relaxation kernel (faster when many cells are chemical),
  * FG_SG_PASS_SEPARATE as a pass of its own before it (faster when few are), FG_SG_PASS_AUTO
  * (default) chooses per relaxation from the chemical cells of an earlier one (separate below
- * 10 %).  The relaxed states and counters are bitwise the same for all three. */
+ * 10 %; it queries an event and copies 32 bytes of counters back behind each relaxation, so set
+ * _FUSED or _SEPARATE before capturing a relaxation into a CUDA graph).  The relaxed states and
+ * counters are bitwise the same for all three. */
 #define FG_SG_PASS_AUTO 0
 #define FG_SG_PASS_FUSED 1
 #define FG_SG_PASS_SEPARATE 2
