@@ -81,13 +81,17 @@ struct fg_solver {
         if (hCntPrev) cudaFreeHost(hCntPrev);
         if (evCnt) cudaEventDestroy(evCnt);
     }
-    // where the surrogate's polish runs (FG_SG_PASS_*).  Automatic: the relaxation counters of
-    // the last surrogate relaxation, copied to pinned host memory behind it (created on the first
-    // one), choose the next one's form once they have arrived
+    // where the surrogate's polish runs (FG_SG_PASS_*).  Automatic: the relaxation counters of a
+    // surrogate relaxation are copied to pinned host memory behind it (buffer and event created
+    // on the first one), one copy in flight at a time; once a copy has arrived, its chemical
+    // cells choose the form (sgAutoPass) that the following relaxations use until the next one
+    // arrives.  The host may run many steps ahead of the device: a copy still in flight keeps the
+    // form chosen before.
     int sgPass = FG_SG_PASS_AUTO;
+    int sgAutoPass = 0;
     int32_t *hCntPrev = nullptr;
     cudaEvent_t evCnt = nullptr;
-    bool cntValid = false;
+    bool cntPending = false;
     // asynchronous uploads copy on their own stream into their own staging buffer, so the copy of
     // the next state overlaps the work queued before it (created on the first asynchronous upload)
     cudaStream_t copyStream = nullptr;
@@ -898,14 +902,16 @@ struct SolverT : public fg_solver {
         // 0.61 against 0.75 ms per relaxation).  The results are bitwise the same either way, so
         // the automatic choice may use whatever counters have reached the host.
         int pass = sgPass == FG_SG_PASS_SEPARATE;
-        if (sg && sgPass == FG_SG_PASS_AUTO) {
+        const bool autoPass = sg && sgPass == FG_SG_PASS_AUTO;
+        if (autoPass) {
             if (!hCntPrev) {
                 FG_CUDA_TRY(cudaHostAlloc((void **)&hCntPrev, 8 * sizeof(int32_t), cudaHostAllocDefault));
                 FG_CUDA_TRY(cudaEventCreateWithFlags(&evCnt, cudaEventDisableTiming));
-            } else if (cntValid && cudaPeekAtLastError() == cudaSuccess) {
+            } else if (cntPending && cudaPeekAtLastError() == cudaSuccess) {
                 const cudaError_t q = cudaEventQuery(evCnt);
                 if (q == cudaSuccess) {
-                    pass = (int64_t)hCntPrev[1] * kSparseChemInv < (int64_t)nU;
+                    sgAutoPass = (int64_t)hCntPrev[1] * kSparseChemInv < (int64_t)nU;
+                    cntPending = false;
                 } else if (q == cudaErrorNotReady) {
                     // not an error: clear it where the query itself left it as the last error
                     if (cudaPeekAtLastError() == cudaErrorNotReady) (void)cudaGetLastError();
@@ -913,6 +919,7 @@ struct SolverT : public fg_solver {
                     return set_err(FG_ERR_CUDA, std::string("relaxation counters: ") + cudaGetErrorString(q));
                 }
             }
+            pass = sgAutoPass;
         }
         const RelaxOrder O{dOrdFlag.as<uint8_t>(), dOrdCnt.as<int32_t>(), dOrdOff.as<int32_t>(), dOrder.as<int32_t>(),
                            dOrdTotal.as<int32_t>(), dPred.as<float4>(), dHullOk.as<int32_t>(), dTcErr.as<int32_t>(),
@@ -922,10 +929,10 @@ struct SolverT : public fg_solver {
         prof_end(s);
         launches += k - 1;
         FG_LAUNCH_CHECK("relaxation");
-        if (sg && sgPass == FG_SG_PASS_AUTO) {
+        if (autoPass && !cntPending) {
             FG_CUDA_TRY(cudaMemcpyAsync(hCntPrev, dCnt.p, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
             FG_CUDA_TRY(cudaEventRecord(evCnt, s));
-            cntValid = true;
+            cntPending = true;
         }
         if (st) {
             FG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1375,7 +1382,6 @@ int fg_solver_set_surrogate_pass(fg_solver *s, int32_t mode) {
     if (mode != FG_SG_PASS_AUTO && mode != FG_SG_PASS_FUSED && mode != FG_SG_PASS_SEPARATE)
         return set_err(FG_ERR_ARG, "fg_solver_set_surrogate_pass: mode is FG_SG_PASS_AUTO, _FUSED or _SEPARATE");
     s->sgPass = mode;
-    s->cntValid = false;
     return FG_OK;
 }
 int fg_relax_stats_read(fg_solver *s, fg_relax_stats *stats) {
